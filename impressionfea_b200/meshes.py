@@ -1,0 +1,183 @@
+"""Synthetic inputs of the forging path: tetrahedral billets and height-field dies.
+
+The reference meshes its billet internally by isosurface stuffing (ThreeD/IsosurfaceStuffing.cs) and builds dies
+from presets (ThreeD/DiePresets3D.cs). The per-iteration path only consumes the resulting arrays, so the cases here
+are generated directly: a seeded 2D Delaunay fill of the quarter disk, extruded in layers, each prism split into
+three tetrahedra by the global-index rule (conforming across shared faces), with node jitter uniform in
++-jitter*h along every direction a node is free to move. The same arrays feed the CUDA path and the oracle.
+"""
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class TetCase:
+    x: np.ndarray          # (nn, 3) float64
+    tets: np.ndarray       # (ne, 4) int32, positively oriented
+    on_x0: np.ndarray      # (nn,) uint8
+    on_y0: np.ndarray      # (nn,) uint8
+    gap0: float            # initial die gap
+    bounds_for_velocity: tuple  # (min_x, min_y, min_z, max_x, max_y) of the seated billet
+
+    @property
+    def nn(self):
+        return len(self.x)
+
+    @property
+    def ne(self):
+        return len(self.tets)
+
+
+@dataclass
+class HeightField:
+    """Rigid die z = h(x, y) on a regular grid (HeightFieldDie): samples (ny+1) x (nx+1), row-major in y."""
+    x0: float
+    y0: float
+    dx: float
+    nx: int
+    ny: int
+    h: np.ndarray
+
+    @staticmethod
+    def flat(z, half_extent=100.0):
+        """Flat die as one grid cell (two triangles)."""
+        return HeightField(-half_extent, -half_extent, 2 * half_extent, 1, 1, np.full(4, float(z)))
+
+    @staticmethod
+    def sample(fn, x0, x1, y0, y1, dx):
+        nx = int(np.ceil((x1 - x0) / dx))
+        ny = int(np.ceil((y1 - y0) / dx))
+        xs = x0 + np.arange(nx + 1) * dx
+        ys = y0 + np.arange(ny + 1) * dx
+        X, Y = np.meshgrid(xs, ys)
+        return HeightField(x0, y0, dx, nx, ny, np.ascontiguousarray(fn(X, Y), np.float64).ravel())
+
+
+def _quarter_disk_points(R, h):
+    """Boundary nodes (on x=0, y=0 and the arc) and hexagonal-lattice interior nodes of the quarter disk."""
+    n_edge = max(2, int(round(R / h)))
+    n_arc = max(2, int(round(0.5 * np.pi * R / h)))
+    pts, kind = [], []  # kind: 0 interior, 1 on y=0 edge, 2 on x=0 edge, 3 on arc, 4 corner
+    pts.append((0.0, 0.0)); kind.append(4)
+    for i in range(1, n_edge):
+        pts.append((R * i / n_edge, 0.0)); kind.append(1)
+    pts.append((R, 0.0)); kind.append(4)
+    for k in range(1, n_arc):
+        th = 0.5 * np.pi * k / n_arc
+        pts.append((R * np.cos(th), R * np.sin(th))); kind.append(3)
+    pts.append((0.0, R)); kind.append(4)
+    for i in range(n_edge - 1, 0, -1):
+        pts.append((0.0, R * i / n_edge)); kind.append(2)
+    dy = h * np.sqrt(3) / 2
+    j = 0
+    y = 0.5 * dy
+    while y < R:
+        xoff = 0.5 * h if j % 2 else 0.0
+        x = 0.5 * h + xoff
+        while x < R:
+            if np.hypot(x, y) < R - 0.45 * h and x > 0.4 * h and y > 0.4 * h:
+                pts.append((x, y)); kind.append(0)
+            x += h
+        y += dy
+        j += 1
+    return np.array(pts), np.array(kind)
+
+
+def quarter_cylinder(R, H, h, z0=0.0, seed=0, jitter=0.1, shut=None):
+    """Quarter-model vertical cylinder (x >= 0, y >= 0), radius R, height H, base at z0, edge length about h.
+
+    Returns a TetCase. With ``shut`` (closed top-die height), gap0 = z0 + H - shut (DieSet3D.Place for flat dies).
+    """
+    from scipy.spatial import Delaunay
+
+    p2, kind = _quarter_disk_points(R, h)
+    tri = Delaunay(p2).simplices.astype(np.int64)
+    a, b, c = p2[tri[:, 0]], p2[tri[:, 1]], p2[tri[:, 2]]
+    area2 = (b[:, 0] - a[:, 0]) * (c[:, 1] - a[:, 1]) - (b[:, 1] - a[:, 1]) * (c[:, 0] - a[:, 0])
+    tri = tri[np.abs(area2) > 1e-12 * h * h]
+    tri.sort(axis=1)
+    nz = max(2, int(round(H / h)))
+    n2 = len(p2)
+    zs = z0 + H * np.arange(nz + 1) / nz
+    nn = n2 * (nz + 1)
+    x = np.zeros((nn, 3))
+    for k in range(nz + 1):
+        x[k * n2:(k + 1) * n2, :2] = p2
+        x[k * n2:(k + 1) * n2, 2] = zs[k]
+    tets = []
+    for k in range(nz):
+        base, top = k * n2, (k + 1) * n2
+        v0, v1, v2 = base + tri[:, 0], base + tri[:, 1], base + tri[:, 2]
+        v3, v4, v5 = top + tri[:, 0], top + tri[:, 1], top + tri[:, 2]
+        tets.append(np.stack([v0, v1, v2, v3], 1))
+        tets.append(np.stack([v1, v2, v3, v4], 1))
+        tets.append(np.stack([v2, v3, v4, v5], 1))
+    tets = np.concatenate(tets).astype(np.int64)
+    # interleave prisms so consecutive tets are spatial neighbours (layer-major order already is)
+    rng = np.random.default_rng(seed)
+    kind3 = np.tile(kind, nz + 1)
+    layer = np.repeat(np.arange(nz + 1), n2)
+    amp = jitter * h
+    d = rng.uniform(-amp, amp, size=(nn, 3))
+    free_z = (layer > 0) & (layer < nz)
+    disp = np.zeros((nn, 3))
+    disp[:, 2] = np.where(free_z, d[:, 2], 0.0)
+    inter = kind3 == 0
+    disp[inter, 0] = d[inter, 0]
+    disp[inter, 1] = d[inter, 1]
+    on_y_edge = kind3 == 1
+    disp[on_y_edge, 0] = d[on_y_edge, 0]
+    on_x_edge = kind3 == 2
+    disp[on_x_edge, 1] = d[on_x_edge, 1]
+    on_arc = kind3 == 3
+
+    def apply(scale):
+        xx = x.copy()
+        xx[:, 2] += disp[:, 2] * scale
+        xx[inter | on_y_edge | on_x_edge, :2] += disp[inter | on_y_edge | on_x_edge, :2] * scale[inter | on_y_edge | on_x_edge, None]
+        th = np.arctan2(x[on_arc, 1], x[on_arc, 0]) + d[on_arc, 0] / R * scale[on_arc]
+        xx[on_arc, 0] = R * np.cos(th)
+        xx[on_arc, 1] = R * np.sin(th)
+        return xx
+
+    scale = np.ones(nn)
+    if jitter > 0:
+        for _ in range(8):
+            xx = apply(scale)
+            det = _tet_det(xx, tets)
+            bad = np.abs(det) < 0.05 * _tet_det(x, tets).__abs__()
+            if not bad.any():
+                break
+            scale[np.unique(tets[bad])] *= 0.5
+        x = apply(scale)
+    det = _tet_det(x, tets)
+    flip = det < 0
+    tets[flip] = tets[flip][:, [0, 2, 1, 3]]
+    det = _tet_det(x, tets)
+    assert (det > 0).all(), "generated mesh has inverted tetrahedra"
+    on_x0 = (x[:, 0] == 0.0).astype(np.uint8)
+    on_y0 = (x[:, 1] == 0.0).astype(np.uint8)
+    gap0 = (z0 + H - shut) if shut is not None else 0.0
+    return TetCase(x=np.ascontiguousarray(x), tets=np.ascontiguousarray(tets.astype(np.int32)), on_x0=on_x0,
+                   on_y0=on_y0, gap0=float(gap0), bounds_for_velocity=(-R, -R, z0, R, R))
+
+
+def _tet_det(x, t):
+    p0 = x[t[:, 0]]
+    a, b, c = x[t[:, 1]] - p0, x[t[:, 2]] - p0, x[t[:, 3]] - p0
+    return np.einsum("ij,ij->i", a, np.cross(b, c))
+
+
+def h_for_tets(R, H, target_tets):
+    """Edge length giving about ``target_tets`` tetrahedra in the quarter cylinder."""
+    area = 0.25 * np.pi * R * R
+    # triangles ~ area / (sqrt(3)/4 h^2), layers ~ H / h, 3 tets per prism
+    return float((3 * area * H / (np.sqrt(3) / 4) / target_tets) ** (1.0 / 3.0))
+
+
+def upset_case_3d(R, H, h, shut, seed=0, jitter=0.1):
+    """Quarter cylinder between flat dies: bottom die z = 0, top die closed at z = shut."""
+    mesh = quarter_cylinder(R, H, h, z0=0.0, seed=seed, jitter=jitter, shut=shut)
+    dies = (HeightField.flat(0.0, 4 * R + 20), HeightField.flat(shut, 4 * R + 20))
+    return mesh, dies
