@@ -1,0 +1,278 @@
+"""Benchmark: stroke increments per second of the 3D upsetting drop-in (plain FP64) on B200.
+
+Workload (one "step" = one forging increment, Forging3DSolver.Step): quarter model of a cylindrical billet
+d = 30 mm, h = 45 mm, ~30k linear tets (seeded Delaunay fill, node jitter +-10 % of h), flat dies as two-triangle
+height fields, C = 150 MPa, eps0 = 0.01, n = 0.1, m = 0.12, friction m_f = 0.4, 40 % height reduction in 80
+increments (ds = 0.225 mm), reference defaults otherwise (ram 50 mm/s, tolerance 1e-3). Synthetic data.
+
+Arms:
+  default            the CUDA path (libifea_gpu.so) — one JSON line, device-timed with CUDA events;
+  --impl reference   the reference algorithm on the host cores (the C# reference cannot run here; its CPU
+                     restatement under oracle/ is timed instead, OpenMP element phase on all host threads).
+
+Multi-GPU: a forging case does not shard (one mesh, one sparse factorisation); N GPUs run N independent replicas
+of the case ("scaling": "weak"), one process per GPU, timing = max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "stroke steps/s on 1 B200, warm-start+FP32 vs plain FP64, at <=0.5% load error"
+UNIT = "stroke steps/s"
+R, H, SHUT_RED, STEPS_TOTAL = 15.0, 45.0, 0.40, 80
+TARGET_TETS = 30000
+
+
+def workload():
+    from impressionfea_b200.config import Forging3DConfig
+    from impressionfea_b200.meshes import h_for_tets, upset_case_3d
+
+    h = round(h_for_tets(R, H, TARGET_TETS), 3)
+    stroke = SHUT_RED * H
+    mesh, dies = upset_case_3d(R, H, h, shut=H - stroke, seed=2024)
+    cfg = Forging3DConfig(C=150, N=0.1, M=0.12, eps0=0.01, friction=0.4, ram=50.0, h=h, ds=stroke / STEPS_TOTAL,
+                          size=H, tol=1e-3)
+    return cfg, mesh, dies
+
+
+def config_dict(cfg, mesh, extra=None):
+    d = {"workload": "3D upsetting drop-in, plain FP64 (quarter cylinder d30 x h45, flat dies, 40% in 80 steps)",
+         "tets": int(mesh.ne), "nodes": int(mesh.nn), "dof": int(3 * mesh.nn), "h_mm": cfg.h, "ds_mm": cfg.ds,
+         "friction": cfg.friction, "tolerance": cfg.tol, "global_batch": 1, "parallelism": "replicas"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index=0):
+        self.samples = []
+        self.index = index
+        self._stop = threading.Event()
+        self._proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                           "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *a):
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if len(s) > 7 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 7 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples if len(s) > 7 for i in range(4) if s[4 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def assembly_algorithmic_bytes(ne, nn, nnz):
+    """Algorithmic bytes of one matrix assembly (conn, gradients, volume, strain, element fields out; velocities,
+    frames; K_vol read, K write, row index; residual and fixed flags)."""
+    ndof = 3 * nn
+    return ne * (16 + 96 + 8 + 8 + 64) + nn * (24 + 72) + nnz * (8 + 8 + 4) + ndof * (8 + 1)
+
+
+def cpu_baseline_sample(budget_s=25.0, threads=None):
+    """Time the CPU restatement on the same workload for a bounded number of increments."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from build_oracle import build_oracle
+    build_oracle()
+    threads = threads or os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import Oracle3D
+    cfg, mesh, dies = workload()
+    o = Oracle3D(cfg, mesh, dies)
+    o.step()  # first increment includes the symbolic analysis; not timed
+    t0 = time.perf_counter()
+    n = 0
+    while n < 50 and time.perf_counter() - t0 < budget_s:
+        o.step()
+        n += 1
+    el = time.perf_counter() - t0
+    return {"value": n / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} increments (steps 2..{n + 1}) of the same workload after one untimed increment; "
+                      f"C restatement, OpenMP element phase, serial scatter and up-looking sparse Cholesky"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    s = cpu_baseline_sample(budget_s=max(20.0, 8.0 * args.steps))
+    cfg, mesh, _ = workload()
+    line = {"impl": "reference", "metric": METRIC, "value": s["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / s["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_dict(cfg, mesh),
+            "cpu_baseline": s, "e2e": {"value": s["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_gpu(args, rank, world):
+    import torch
+
+    from impressionfea_b200.forging3d import Forging3DSolver
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    cfg, mesh, dies = workload()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    s = Forging3DSolver(cfg, mesh, dies)
+    s.set_stream(stream.cuda_stream)
+    for _ in range(args.warmup):
+        s.step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    durs, infos = [], []
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            if s.IsFinished:
+                break
+            flush.zero_()  # L2 flush between timed increments (outside the timed pair)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            infos.append(s.step())
+            b.record(stream)
+            b.synchronize()
+            durs.append(a.elapsed_time(b))
+    torch.cuda.synchronize()
+    k = len(durs)
+    total_ms = float(sum(durs))
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+        torch.distributed.barrier()
+    value = world * k / (total_ms / 1000.0)
+
+    # roofline of the dominant kernel of this library: the matrix assembly (element + column kernels)
+    nnz = int(s.scalar("nnz"))
+    s.prepare_step()
+    for _ in range(3):
+        s.assemble(1, 1)
+    asm = []
+    for _ in range(10):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s.assemble(1, 1)
+        b.record(stream)
+        b.synchronize()
+        asm.append(a.elapsed_time(b))
+    asm_ms = float(np.median(asm))
+    abytes = assembly_algorithmic_bytes(mesh.ne, mesh.nn, nnz)
+    peak, peak_kind = measured_peak()
+    achieved = abytes / (asm_ms / 1000.0) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "assembly_traffic.json")
+    if os.path.exists(tp):
+        try:
+            with open(tp) as f:
+                traffic = json.load(f).get("bytes_per_assembly")
+        except Exception:
+            traffic = None
+
+    # end to end through the public API with host buffers: mesh/die upload, K increments, snapshot read-back
+    e2e_steps = min(args.steps, 10)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s2 = Forging3DSolver(cfg, mesh, dies)
+    d2h = 0
+    for _ in range(e2e_steps):
+        s2.step()
+        for nm in ("x", "vg", "contact", "eps", "dmg", "el_sig", "el_rate", "el_mean"):
+            d2h += s2.array(nm).nbytes
+    e2e_s = time.perf_counter() - t0
+    s2.close()
+    h2d = mesh.x.nbytes + mesh.tets.nbytes + mesh.on_x0.nbytes + mesh.on_y0.nbytes + sum(d.h.nbytes for d in dies)
+
+    gpu_launches = None
+    if rank == 0:
+        clocks = clk.summary()
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": k, "warmup": args.warmup,
+                "ms_per_step": total_ms / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": config_dict(cfg, mesh, {"l2": "flushed (256 MiB write) between timed increments",
+                                                  "newton_iterations": int(sum(i["iterations"] for i in infos)),
+                                                  "factorisations": int(infos[-1]["n_factor"]) if infos else 0,
+                                                  "pcg_solves": int(infos[-1]["n_pcg"]) if infos else 0,
+                                                  "load_last_N": infos[-1]["load"] if infos else None}),
+                "roofline": {"kernel": "assembly (k_element<MATRIX> + k_columns<MATRIX,BC>)", "bound": "hbm",
+                             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                             "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes": abytes,
+                             "ms_per_launch": asm_ms},
+                "e2e": {"value": e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
+                        "d2h_bytes_per_step": d2h / e2e_steps},
+                "gpu_launches": gpu_launches, "clocks": clocks}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_sample(budget_s=args.cpu_budget)
+        print(json.dumps(line))
+    s.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=25.0)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_gpu(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

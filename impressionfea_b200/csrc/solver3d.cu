@@ -1,0 +1,888 @@
+// solver3d.cu — host orchestration of the 3D forging increment on the GPU and its C ABI (ifea3d_*).
+//
+// The control flow is Forging3DSolver's (ThreeD/Forging3DSolver.cs:540-1537): the host runs the increment
+// loop, the Newton iteration, the line search and the PCG loop, and reads back only the handful of scalars
+// those decisions need; every array operation is a device kernel on the context's stream.
+#include <climits>
+#include <cstdarg>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels3d.cuh"
+#include "mesh3d.h"
+#include "runtime.cuh"
+#include "spd.cuh"
+
+namespace ifea {
+
+static std::string fmt(const char *f, ...) __attribute__((format(printf, 1, 2)));
+static std::string fmt(const char *f, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, f);
+    vsnprintf(buf, sizeof buf, f, ap);
+    va_end(ap);
+    return buf;
+}
+
+struct Forging3D {
+    ifea3d_params P;
+    cudaStream_t st = nullptr;
+    std::string err;
+    // constants (Forging3DSolver.cs:137-150)
+    double rate_ref = 0, rate_cut = 0, sig_ref = 0, k_pen = 0, u0 = 0, h = 0;
+    // increment state
+    double gap0 = 0, gap = 0, ds_cur = 0, time = 0, last_rel = INFINITY, vol0 = 0;
+    int step_index = 0, warm = 0, recovery_pass = 0;
+    bool have_vg_prev = false, initialized = false;
+    int iterations = 0, n_fact = 0, n_pcg = 0, remesh_requests = 0, projection_reverts = 0, corner_penetrations = 0;
+    int last_cutbacks = 0, n_newton = 0, n_assemble = 0, lin_its = 0;
+    double load = 0, reaction = 0, power = 0, last_dt = 0, rnorm = 0, beta_last = 0, max_diag = 0;
+    // linear solver (SolveLinear :965-1019)
+    std::unique_ptr<GpuSpd> lin;
+    bool need_analyze = true, have_factor = false;
+    int pcg_failures = 0, pcg_skip = 0;
+    // mesh
+    TetTopology topo;
+    int have_dies = 0;
+    HField die[2];
+    DBuf<double> die_h[2];
+    // device arrays
+    DBuf<int32_t> d_tets, d_nts, d_ntl, d_qk, d_gslot, d_bface, d_bowner, d_nfs, d_nfl, d_nbr_start, d_nbr, d_diag,
+        d_gstart, d_gnode, d_kvs, d_kvn, d_kvpj, d_kvks, d_kvk, d_nfix, d_dieaxis, d_err, d_counters;
+    DBuf<int8_t> d_ntl_local;
+    DBuf<uint8_t> d_bsym, d_surf, d_onx, d_ony, d_fixed, d_contact, d_release, d_cT, d_bad;
+    DBuf<double> d_hloc, d_x, d_xT, d_vg, d_vgprev, d_ax, d_fixedval, d_kfric, d_afric, d_grad, d_vol, d_vnode,
+        d_gcoef, d_clocal, d_kvol, d_val, d_eps, d_dmg, d_elsig, d_elrate, d_eldev, d_elmean, d_vbuf[2], d_r, d_b,
+        d_dv, d_er, d_eg, d_ew, d_eenergy, d_epower, d_partials, d_scalars, d_nrm, d_pred, d_nodal, d_q, d_pr, d_pz,
+        d_pp, d_pq;
+    int vcur = 0;
+    HostPinned<double> hs;
+    HostPinned<int32_t> hi;
+    int wpb = 8;          // warps per block of the column kernels
+    size_t col_smem = 0;  // dynamic shared memory of the column kernels
+
+    Forging3D(const ifea3d_params &p) : P(p)
+    {
+        cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+        h = P.h;
+        ds_cur = P.ds;
+        rate_ref = P.ram / P.size;
+        rate_cut = 1e-3 * rate_ref;
+        sig_ref = flow_stress(P.C, P.N, P.M, P.eps0, 0, rate_ref);
+        k_pen = P.penalty_factor * sig_ref / rate_ref;
+        u0 = 5e-3 * P.ram;
+        hs.resize(S_COUNT + 8);
+        hi.resize(8);
+        d_partials.resize((size_t)S_COUNT * kReduceBlocks);
+        d_scalars.resize(S_COUNT);
+        d_err.resize(4);
+        d_counters.resize(4);
+        lin.reset(new GpuSpd(st));
+    }
+    bool own_stream = true;
+    ~Forging3D()
+    {
+        if (st) cudaStreamSynchronize(st);
+        lin.reset();
+        if (st && own_stream) cudaStreamDestroy(st);
+    }
+
+    // Run on a caller-provided stream from now on (the context's own stream is kept for destruction order).
+    void set_stream(cudaStream_t s)
+    {
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        if (own_stream) cudaStreamDestroy(st);
+        own_stream = false;
+        st = s;
+        lin->set_stream(s);
+    }
+
+    int grid(int n) const { return std::max(1, std::min((n + 255) / 256, 8 * 148)); }
+
+    View3 view()
+    {
+        View3 V;
+        memset(&V, 0, sizeof V);
+        V.nn = topo.nn; V.ne = topo.ne; V.ndof = topo.ndof; V.nbf = (int)topo.bowner.size();
+        V.tets = d_tets; V.nts = d_nts; V.ntl = d_ntl; V.qk = d_qk; V.gslot = d_gslot; V.bface = d_bface;
+        V.bowner = d_bowner; V.nfs = d_nfs; V.nfl = d_nfl; V.ntl_local = d_ntl_local; V.bsym = d_bsym;
+        V.is_surface = d_surf; V.on_x0 = d_onx; V.on_y0 = d_ony; V.nbr_start = d_nbr_start; V.nbr = d_nbr;
+        V.diag_slot = d_diag; V.g_start = d_gstart; V.g_node = d_gnode; V.kv_start = d_kvs; V.kv_n = d_kvn;
+        V.kv_pj = d_kvpj; V.kv_kstart = d_kvks; V.kv_k = d_kvk; V.h_local = d_hloc;
+        V.x = d_x; V.vg = d_vg; V.vg_prev = d_vgprev; V.ax = d_ax; V.fixed_val = d_fixedval; V.k_fric = d_kfric;
+        V.a_fric = d_afric; V.grad = d_grad; V.vol = d_vol; V.v_node = d_vnode; V.g_coef = d_gcoef; V.c_local = d_clocal;
+        V.kvol = d_kvol; V.val = d_val; V.eps = d_eps; V.dmg = d_dmg; V.el_sig = d_elsig; V.el_rate = d_elrate;
+        V.el_dev = d_eldev; V.el_mean = d_elmean; V.v = d_vbuf[vcur]; V.v_trial = d_vbuf[1 - vcur]; V.r = d_r; V.b = d_b;
+        V.dv = d_dv; V.e_r = d_er; V.e_g = d_eg; V.e_w = d_ew; V.e_energy = d_eenergy; V.e_power = d_epower;
+        V.n_fix = d_nfix; V.die_axis = d_dieaxis; V.fixed = d_fixed; V.contact = d_contact; V.release = d_release;
+        V.partials = d_partials; V.scalars = d_scalars; V.err = d_err;
+        V.die[0] = die[0]; V.die[1] = die[1];
+        V.C = P.C; V.N = P.N; V.M = P.M; V.eps0 = P.eps0; V.friction = P.friction; V.ram = P.ram;
+        V.rate_cut = rate_cut; V.k_pen = k_pen; V.u0 = u0; V.newton_blend = P.newton_blend; V.gap = gap;
+        return V;
+    }
+
+    // ---------------------------------------------------------------- reductions / readback
+    void finalize(std::initializer_list<int> codes)
+    {
+        SlotList l;
+        l.n = 0;
+        for (int c : codes) l.code[l.n++] = c;
+        k_finalize<<<l.n, 256, 0, st>>>(d_partials, d_scalars, l);
+    }
+    static int MAXS(int slot) { return slot | (1 << 16); }
+    const double *read_scalars()
+    {
+        cuda_check(cudaMemcpyAsync(hs.p, d_scalars.p, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H scalars");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        return hs.p;
+    }
+    void reset_err()
+    {
+        int32_t v[4] = {INT_MAX, INT_MAX, 0, 0};
+        cuda_check(cudaMemcpyAsync(d_err.p, v, sizeof v, cudaMemcpyHostToDevice, st), "H2D err");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    }
+    void read_err(int32_t *out4)
+    {
+        cuda_check(cudaMemcpyAsync(hi.p, d_err.p, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "D2H err");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        memcpy(out4, hi.p, 4 * sizeof(int32_t));
+    }
+
+    // ---------------------------------------------------------------- setup
+    void set_mesh(int nn, int ne, const double *x, const int32_t *tets, const uint8_t *ox, const uint8_t *oy)
+    {
+        std::string e = topo.build(nn, ne, x, tets, ox, oy);
+        if (!e.empty()) throw Failure(IFEA_INPUT_INVALID, e);
+        std::vector<double> hl = local_lengths(topo, x, h);
+        d_tets.upload(topo.tets, st); d_nts.upload(topo.nts, st); d_ntl.upload(topo.ntl, st); d_qk.upload(topo.qk, st);
+        d_gslot.upload(topo.gslot, st); d_bface.upload(topo.bface, st); d_bowner.upload(topo.bowner, st);
+        d_nfs.upload(topo.nfs, st); d_nfl.upload(topo.nfl, st); d_ntl_local.upload(topo.ntl_local, st);
+        d_bsym.upload(topo.bsym, st); d_surf.upload(topo.is_surface, st); d_onx.upload(topo.on_x0, st);
+        d_ony.upload(topo.on_y0, st); d_nbr_start.upload(topo.nbr_start, st); d_nbr.upload(topo.nbr, st);
+        d_diag.upload(topo.diag_slot, st); d_gstart.upload(topo.g_start, st); d_gnode.upload(topo.g_node, st);
+        d_kvs.upload(topo.kv_start, st); d_kvn.upload(topo.kv_n, st); d_kvpj.upload(topo.kv_pj, st);
+        d_kvks.upload(topo.kv_kstart, st); d_kvk.upload(topo.kv_k, st); d_hloc.upload(hl, st);
+        d_x.upload(x, 3 * (size_t)nn, st);
+        size_t N3 = 3 * (size_t)nn, ndof = topo.ndof, G = topo.g_node.size();
+        d_xT.resize(N3); d_vg.resize(N3); d_vgprev.resize(N3); d_ax.resize(9 * (size_t)nn); d_fixedval.resize(ndof);
+        d_kfric.resize(nn); d_afric.resize(nn); d_grad.resize(12 * (size_t)ne); d_vol.resize(ne); d_vnode.resize(nn);
+        d_gcoef.resize(3 * G); d_clocal.resize(3 * G); d_kvol.resize(topo.nnz); d_val.resize(topo.nnz);
+        d_eps.resize(ne); d_dmg.resize(ne); d_elsig.resize(ne); d_elrate.resize(ne); d_eldev.resize(6 * (size_t)ne);
+        d_elmean.resize(ne); d_vbuf[0].resize(ndof); d_vbuf[1].resize(ndof); d_r.resize(ndof); d_b.resize(ndof);
+        d_dv.resize(ndof); d_er.resize(12 * (size_t)ne); d_eg.resize(12 * (size_t)ne); d_ew.resize(2 * (size_t)ne);
+        d_eenergy.resize(ne); d_epower.resize(ne); d_nrm.resize(N3); d_pred.resize(N3); d_nodal.resize(nn);
+        d_q.resize(ne); d_pr.resize(ndof); d_pz.resize(ndof); d_pp.resize(ndof); d_pq.resize(ndof);
+        d_nfix.resize(nn); d_dieaxis.resize(nn); d_fixed.resize(ndof); d_contact.resize(nn); d_release.resize(nn);
+        d_cT.resize(nn); d_bad.resize(nn);
+        for (auto *b : {&d_vg, &d_vgprev, &d_eps, &d_dmg, &d_elmean, &d_eldev, &d_vbuf[0], &d_vbuf[1], &d_r, &d_b, &d_dv})
+            b->zero(st);
+        d_contact.zero(st); d_release.zero(st); d_fixed.zero(st); d_fixedval.zero(st); d_nfix.zero(st);
+        d_dieaxis.zero(st); d_kvol.zero(st); d_val.zero(st);
+        std::vector<double> sig(ne, sig_ref);
+        d_elsig.upload(sig, st);
+        d_elrate.zero(st);
+        // column-kernel launch shape: chunk of 9*max_nbr doubles per warp in shared memory
+        size_t per_warp = 9 * (size_t)topo.max_nbr * sizeof(double);
+        wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (160 * 1024) / std::max<size_t>(per_warp, 1)));
+        col_smem = per_warp * wpb;
+        if (per_warp > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "node neighbourhood too large for the column kernel");
+        auto set_smem = [&](const void *f) {
+            cuda_check(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem), "cudaFuncSetAttribute");
+        };
+        set_smem((const void *)k_columns<ASM_MATRIX, true>);
+        set_smem((const void *)k_columns<ASM_MATRIX, false>);
+        set_smem((const void *)k_columns<ASM_RESIDUAL, false>);
+        set_smem((const void *)k_columns<ASM_ENERGY, false>);
+        set_smem((const void *)k_kvol);
+        need_analyze = true;
+        have_factor = false;
+        pcg_failures = pcg_skip = 0;
+        vcur = 0;
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    }
+
+    void set_die(int side, int nx, int ny, double x0, double y0, double dx, const double *hh)
+    {
+        if (side < 0 || side > 1 || nx < 1 || ny < 1 || !(dx > 0)) throw Failure(IFEA_INPUT_INVALID, "invalid die grid");
+        die_h[side].upload(hh, (size_t)(nx + 1) * (ny + 1), st);
+        die[side].side = side; die[side].nx = nx; die[side].ny = ny;
+        die[side].x0 = x0; die[side].y0 = y0; die[side].dx = dx; die[side].h = die_h[side].p;
+        have_dies |= 1 << side;
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    }
+
+    double volume()
+    {
+        View3 V = view();
+        k_volume<<<kReduceBlocks, 256, 0, st>>>(V);
+        finalize({S_VOLUME});
+        return read_scalars()[S_VOLUME] * P.sym_factor;
+    }
+
+    // Constructor tail (Forging3DSolver.cs:156-184)
+    void init(double g0, double min_x, double min_y, double min_z, double max_x, double max_y)
+    {
+        if (have_dies != 3 || topo.nn == 0) throw Failure(IFEA_INPUT_INVALID, "mesh and both dies must be set first");
+        gap0 = gap = g0;
+        View3 V = view();
+        int nn = topo.nn;
+        std::vector<double> cb(nn), ct(nn);
+        d_pred.resize(3 * (size_t)nn);
+        k_initial_contact<<<grid(nn), 256, 0, st>>>(V, 0.05 * h, d_pred.p, d_pred.p + nn);
+        std::vector<uint8_t> contact(nn);
+        d_contact.download(contact.data(), nn, st);
+        cuda_check(cudaMemcpyAsync(cb.data(), d_pred.p, nn * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        cuda_check(cudaMemcpyAsync(ct.data(), d_pred.p + nn, nn * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        int nb = 0, ntop = 0;
+        for (int n = 0; n < nn; n++) { nb += contact[n] == IFEA_BOTTOM_DIE; ntop += contact[n] == IFEA_TOP_DIE; }
+        // ForceContact (:366-378): the surface node with the smallest clearance, first on ties
+        auto force = [&](int side, const std::vector<double> &c) {
+            int best = -1;
+            double bc = DBL_MAX;
+            for (int n = 0; n < nn; n++)
+                if (topo.is_surface[n] && c[n] < bc) { bc = c[n]; best = n; }
+            if (best >= 0) contact[best] = (uint8_t)side;
+        };
+        if (nb == 0) force(IFEA_BOTTOM_DIE, cb);
+        if (ntop == 0) force(IFEA_TOP_DIE, ct);
+        d_contact.upload(contact, st);
+        k_place_and_velocity<<<grid(nn), 256, 0, st>>>(V, rate_ref, 0, 0, 0);
+        k_initial_velocity<<<grid(nn), 256, 0, st>>>(V, rate_ref, 0.5 * (min_x + max_x), 0.5 * (min_y + max_y), min_z);
+        vol0 = volume();
+        initialized = true;
+    }
+
+    // ---------------------------------------------------------------- PrepareStep (:660-758)
+    void prepare_step()
+    {
+        View3 V = view();
+        reset_err();
+        k_frames<<<grid(topo.nn), 256, 0, st>>>(V);
+        k_grad<<<grid(topo.ne), 256, 0, st>>>(V);
+        int32_t e4[4];
+        read_err(e4);
+        if (e4[0] != INT_MAX) throw Failure(IFEA_MESH_DISTORTED, fmt("Tetrahedron %d is inverted at step %d.", e4[0], step_index));
+        k_anp_coef<<<grid(topo.nn), 256, 0, st>>>(V);
+        int G = (int)topo.g_node.size();
+        k_clocal<<<grid(G), 256, 0, st>>>(V, G);
+        k_kvol<<<std::min(kReduceBlocks * 2, (topo.nn + wpb - 1) / wpb), wpb * 32, col_smem, st>>>(V, topo.max_nbr);
+        k_friction_prep<<<grid(topo.nn), 256, 0, st>>>(V);
+        int trend = P.extrapolate_start && warm && have_vg_prev;
+        k_guess<<<grid(topo.nn), 256, 0, st>>>(V, trend);
+        cuda_check(cudaGetLastError(), "prepare_step launch");
+    }
+
+    // ---------------------------------------------------------------- Assemble (:1115-1217)
+    // Returns energy; power via *pw. bc: apply the BC pass inside the column kernel (MATRIX only).
+    double assemble(int mode, int newton, const double *v, bool bc, double *pw)
+    {
+        n_assemble++;
+        View3 V = view();
+        switch (mode) {
+        case ASM_MATRIX: k_element<ASM_MATRIX><<<kReduceBlocks, 256, 0, st>>>(V, v, newton); break;
+        case ASM_RESIDUAL: k_element<ASM_RESIDUAL><<<kReduceBlocks, 256, 0, st>>>(V, v, newton); break;
+        default: k_element<ASM_ENERGY><<<kReduceBlocks, 256, 0, st>>>(V, v, newton); break;
+        }
+        int cb = kReduceBlocks;
+        if (mode == ASM_MATRIX && bc) k_columns<ASM_MATRIX, true><<<cb, wpb * 32, col_smem, st>>>(V, v, newton, topo.max_nbr);
+        else if (mode == ASM_MATRIX) k_columns<ASM_MATRIX, false><<<cb, wpb * 32, col_smem, st>>>(V, v, newton, topo.max_nbr);
+        else if (mode == ASM_RESIDUAL) k_columns<ASM_RESIDUAL, false><<<cb, wpb * 32, 0, st>>>(V, v, newton, topo.max_nbr);
+        else k_columns<ASM_ENERGY, false><<<cb, wpb * 32, 0, st>>>(V, v, newton, topo.max_nbr);
+        cuda_check(cudaGetLastError(), "assemble launch");
+        finalize({S_E_VOL, S_E_ELEM, S_E_FRIC, S_P_ELEM, S_P_FRIC, S_RNORM2, MAXS(S_MAXDIAG)});
+        const double *s = read_scalars();
+        double energy = s[S_E_VOL] + s[S_E_ELEM] + s[S_E_FRIC];
+        if (pw) *pw = 2 * s[S_E_VOL] + s[S_P_ELEM] + s[S_P_FRIC];
+        if (mode == ASM_MATRIX && bc) {
+            max_diag = s[S_MAXDIAG];
+            rnorm = sqrt(s[S_RNORM2]);
+        }
+        return energy;
+    }
+
+    void apply_bc_separately()
+    {
+        View3 V = view();
+        k_apply_bc<<<kReduceBlocks, 256, 0, st>>>(V);
+        finalize({MAXS(S_MAXDIAG)});
+        k_regularise<<<grid(topo.ndof), 256, 0, st>>>(V);
+        max_diag = read_scalars()[S_MAXDIAG];
+    }
+
+    // ---------------------------------------------------------------- SolveLinear (:965-1019) and Pcg (:1051-1087)
+    double dot_read(const double *a, const double *b, int slot, const double *c = nullptr, int slot2 = S_NORM_B,
+                    double *second = nullptr)
+    {
+        View3 V = view();
+        k_dot2<<<kReduceBlocks, 256, 0, st>>>(V, a, b, slot, c, slot2);
+        if (c) finalize({slot, slot2}); else finalize({slot});
+        const double *s = read_scalars();
+        if (second) *second = s[slot2];
+        return s[slot];
+    }
+
+    int pcg(const double *b, double *x, double tol, int max_it)
+    {
+        View3 V = view();
+        int n = topo.ndof;
+        double bb = dot_read(b, b, S_BB);
+        double bnorm = sqrt(bb);
+        if (bnorm == 0) {
+            cuda_check(cudaMemsetAsync(x, 0, n * sizeof(double), st), "memset");
+            return 0;
+        }
+        int sp_grid = std::min(kReduceBlocks * 4, (topo.nn * 32 + 255) / 256);
+        lin->solve(b, x);
+        k_spmv<<<sp_grid, 256, 0, st>>>(V, x, d_pq);
+        k_pcg_residual<<<grid(n), 256, 0, st>>>(n, b, d_pq, d_pr);
+        lin->solve(d_pr, d_pz);
+        cuda_check(cudaMemcpyAsync(d_pp.p, d_pz.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st), "D2D");
+        k_dot2<<<kReduceBlocks, 256, 0, st>>>(V, d_pr, d_pz, S_RZ, d_pr, S_RR);
+        finalize({S_RZ, S_RR});
+        double rr = read_scalars()[S_RR];
+        for (int it = 0; it < max_it; it++) {
+            if (sqrt(rr) <= tol * bnorm) return it;
+            k_spmv<<<sp_grid, 256, 0, st>>>(V, d_pp, d_pq);
+            k_dot2<<<kReduceBlocks, 256, 0, st>>>(V, d_pp, d_pq, S_PQ, nullptr, 0);
+            finalize({S_PQ});
+            k_pcg_xr<<<grid(n), 256, 0, st>>>(n, d_scalars, x, d_pr, d_pp, d_pq);
+            lin->solve(d_pr, d_pz);
+            k_dot2<<<kReduceBlocks, 256, 0, st>>>(V, d_pr, d_pz, S_RZNEW, d_pr, S_RR);
+            finalize({S_RZNEW, S_RR});
+            k_pcg_p<<<grid(n), 256, 0, st>>>(n, d_scalars, d_pp, d_pz);
+            k_pcg_roll<<<1, 1, 0, st>>>(d_scalars);
+            rr = read_scalars()[S_RR];
+            lin_its++;
+        }
+        return sqrt(rr) <= tol * bnorm ? max_it : -1;
+    }
+
+    // b -> x; returns 0 for PCG, 1 for a fresh factorisation
+    int solve_linear(const double *b, double *x)
+    {
+        if (have_factor && pcg_skip > 0) {
+            pcg_skip--;
+        } else if (have_factor) {
+            int its = pcg(b, x, 1e-7, P.pcg_budget);
+            if (its >= 0) {
+                pcg_failures = 0;
+                n_pcg++;
+                return 0;
+            }
+            if (++pcg_failures >= 2) pcg_skip = std::min(64, 1 << (pcg_failures - 1));
+        }
+        if (need_analyze) {
+            lin->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3);
+            need_analyze = false;
+        }
+        try {
+            lin->factorize(d_val);
+            lin->solve(b, x);
+            lin->check_finite(x);
+        } catch (Failure &f) {
+            have_factor = false;
+            if (f.status == IFEA_NOT_SPD) throw;
+            throw Failure(IFEA_DIVERGED, fmt("Sparse factorisation failed at step %d (cuSOLVER csrchol): %s", step_index, f.what()));
+        }
+        have_factor = true;
+        n_fact++;
+        return 1;
+    }
+
+    // ---------------------------------------------------------------- SolveVelocity (:875-948)
+    int solve_velocity(bool *converged, const volatile int32_t *cancel)
+    {
+        *converged = false;
+        last_rel = INFINITY;
+        int it, halved = 0;
+        bool secant_only = false;
+        const int newton_limit = 20;
+        int n = topo.ndof;
+        for (it = 1; it <= P.max_iter; it++) {
+            if (cancel && *cancel) throw Failure(IFEA_CANCELLED, "The operation was canceled.");
+            if (P.sticky_secant && halved >= 2) secant_only = true;
+            int newton = (warm || it > 2) && it <= newton_limit && !secant_only && !(P.adaptive_newton && halved >= 2);
+            n_newton += newton;
+            double e0 = assemble(ASM_MATRIX, newton, d_vbuf[vcur], true, nullptr);
+            {
+                View3 V = view();
+                k_regularise<<<grid(n), 256, 0, st>>>(V);
+            }
+            solve_linear(d_b, d_dv);
+            // slope = sum R.dv with R fixed-zeroed (= -b.dv), and |dv|^2
+            double dvdv = 0;
+            double slope = -dot_read(d_b, d_dv, S_DOT, d_dv, S_NORM_B, &dvdv);
+            double beta = 1;
+            for (int ls = 0; ls < 8; ls++) {
+                k_axpy<<<grid(n), 256, 0, st>>>(n, d_vbuf[1 - vcur], d_vbuf[vcur], d_dv, beta);
+                double e1 = assemble(ASM_ENERGY, 0, d_vbuf[1 - vcur], false, nullptr);
+                if (e1 <= e0 + 1e-4 * beta * slope + 1e-11 * fabs(e0)) break;
+                double curv = (e1 - e0 - slope * beta) / (beta * beta);
+                beta = P.quadratic_ls && curv > 0 ? rclamp(-slope / (2 * curv), 0.1 * beta, 0.7 * beta) : 0.5 * beta;
+            }
+            vcur = 1 - vcur;
+            halved = newton && beta < 1 ? halved + 1 : 0;
+            double vv = dot_read(d_vbuf[vcur], d_vbuf[vcur], S_NORM_A);
+            double rel = beta * sqrt(dvdv) / rmax(sqrt(vv), 1e-30);
+            last_rel = rel;
+            beta_last = beta;
+            if (std::isnan(rel)) throw Failure(IFEA_DIVERGED, fmt("Velocity solution became NaN at step %d.", step_index));
+            if (rel < P.tol) {
+                *converged = true;
+                return it;
+            }
+        }
+        return it - 1;
+    }
+
+    // ---------------------------------------------------------------- FinalEvaluation (:1402-1451)
+    double final_evaluation(double *reaction_out)
+    {
+        double pw = 0;
+        assemble(ASM_RESIDUAL, 0, d_vbuf[vcur], false, &pw);
+        View3 V = view();
+        k_final_nodes<<<kReduceBlocks, 256, 0, st>>>(V);
+        finalize({S_REACTION, MAXS(S_MAX_B), MAXS(S_MAX_T)});
+        k_release<<<kReduceBlocks, 256, 0, st>>>(V);
+        finalize({S_KEPT_B, S_KEPT_T});
+        k_release_keep<<<grid(topo.nn), 256, 0, st>>>(V);
+        k_nodal_mean<<<grid(topo.nn), 256, 0, st>>>(V, d_nodal);
+        k_el_mean<<<grid(topo.ne), 256, 0, st>>>(V, d_nodal);
+        const double *s = read_scalars();
+        have_vg_prev = true;
+        reaction = s[S_REACTION];
+        if (reaction_out) *reaction_out = reaction;
+        power = pw;
+        return pw;
+    }
+
+    // ---------------------------------------------------------------- TryUpdate (:1455-1537)
+    double min_quality(const double *x)
+    {
+        View3 V = view();
+        k_quality_check<<<kReduceBlocks, 256, 0, st>>>(V, x, -INFINITY);
+        finalize({MAXS(S_MINQ)});
+        return -read_scalars()[S_MINQ];
+    }
+
+    int smooth_interior(double *x, double qtarget, int sweeps)
+    {
+        View3 V = view();
+        d_counters.zero(st);
+        k_smooth_interior<<<1, 32, 0, st>>>(V, x, qtarget, sweeps, d_bad, d_counters.p + 2);
+        int32_t c[4];
+        d_counters.download(c, 4, st);
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        return c[2];
+    }
+
+    bool try_update(double dt, std::string &why)
+    {
+        double gapT = rmax(0, gap - P.ram * dt);
+        if (gapT < 1e-9) gapT = 0;
+        View3 V = view();
+        int nn = topo.nn;
+        bool lenient = recovery_pass >= 2;
+        k_surface_normals<<<grid(nn), 256, 0, st>>>(V, d_x, d_nrm);
+        k_predict<<<kReduceBlocks, 256, 0, st>>>(V, dt, gapT, h, lenient, d_xT, d_pred, d_cT);
+        finalize({MAXS(S_MAXPEN)});
+        double maxPenRel = read_scalars()[S_MAXPEN];
+        if (maxPenRel > 0.5) {
+            why = "die penetration exceeds half the local element size";
+            return false;
+        }
+        if (min_quality(d_xT) < 0.05) {
+            static const double ladder[2] = {0.05, 0.1};
+            double frac = ladder[iclamp(recovery_pass, 0, 1)];
+            d_counters.zero(st);
+            k_improve_placement<<<1, 32, 0, st>>>(V, d_xT, d_cT, d_pred, d_nrm, gapT, 0.05, h, lenient, frac, d_counters);
+            int32_t c[4];
+            d_counters.download(c, 4, st);
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+            projection_reverts += c[0];
+            corner_penetrations += c[1];
+            if (min_quality(d_xT) < 0.05) smooth_interior(d_xT, 0.05, 6);
+        }
+        reset_err();
+        k_quality_check<<<kReduceBlocks, 256, 0, st>>>(V, d_xT, 0.005);
+        int32_t e4[4];
+        read_err(e4);
+        if (e4[1] != INT_MAX) {
+            why = fmt("tetrahedron %d collapsed", e4[1]);
+            return false;
+        }
+        std::swap(d_x.p, d_xT.p);
+        std::swap(d_contact.p, d_cT.p);
+        gap = gapT;
+        time += dt;
+        return true;
+    }
+
+    // ---------------------------------------------------------------- Step (:540-638)
+    void step(ifea_step_info *info, const volatile int32_t *cancel)
+    {
+        if (!initialized) throw Failure(IFEA_BAD_STATE, "ifea3d_init must be called before stepping.");
+        if (gap <= 1e-9) throw Failure(IFEA_BAD_STATE, "Simulation already reached the closed-die position.");
+        step_index++;
+        // RemeshTrigger (:1867-1883): first-aid smoothing; a remesh itself is out of scope and only counted
+        double rq = P.remesh_quality;
+        if (min_quality(d_x) < rq) smooth_interior(d_x, rq, 6);
+        if (min_quality(d_x) < rq) remesh_requests++;
+        else {
+            View3 V = view();
+            k_edges_layers<<<kReduceBlocks, 256, 0, st>>>(V);
+            finalize({MAXS(S_MAXEDGE), MAXS(S_THIN)});
+            if (read_scalars()[S_MAXEDGE] > 2.8 * h) remesh_requests++;
+        }
+        double step_cap = P.ds * h / P.h;
+        int its = 0, used_cutback = 0;
+        bool ok = false;
+        double dt = 0;
+        std::string why;
+        const int passes = 4;
+        for (int pass = 0; pass < passes && !ok; pass++) {
+            recovery_pass = pass;
+            prepare_step();
+            bool converged = false;
+            its = solve_velocity(&converged, cancel);
+            if (!converged) {
+                if (!(last_rel < 1e-2)) {
+                    if (pass < passes - 1) remesh_requests++;
+                    throw Failure(IFEA_DIVERGED, fmt("Velocity solution did not converge at step %d (stroke %.3f mm): |dv|/|v| = %.2e.",
+                                                     step_index, gap0 - gap, last_rel));
+                }
+            }
+            double pw = final_evaluation(&reaction);
+            load = pw / P.ram * P.sym_factor;
+            reaction *= P.sym_factor;
+            View3 V = view();
+            k_edges_layers<<<kReduceBlocks, 256, 0, st>>>(V);
+            finalize({MAXS(S_MAXEDGE), MAXS(S_THIN)});
+            double thin_neg = read_scalars()[S_THIN];
+            double thinnest = std::isfinite(thin_neg) ? -thin_neg : INFINITY;
+            double layer = std::isfinite(thinnest) ? rmax(0.1 * thinnest, step_cap / (1 << P.max_cutbacks)) : INFINITY;
+            double ds = rmin(P.auto_step ? rmin(ds_cur, step_cap) : step_cap, layer);
+            dt = rmin(ds, gap) / P.ram;
+            if (gap - P.ram * dt < 0.05 * ds) dt = gap / P.ram;
+            for (int attempt = 0; attempt <= P.max_cutbacks && !ok; attempt++) {
+                double dta = dt / (1 << attempt);
+                ok = try_update(dta, why);
+                if (ok) {
+                    dt = dta;
+                    used_cutback = attempt;
+                }
+            }
+            if (ok || pass == passes - 1) break;
+            remesh_requests++;  // Remesh(...) would run here; unavailable, so the ladder continues
+        }
+        recovery_pass = 0;
+        if (!ok)
+            throw Failure(IFEA_MESH_DISTORTED, fmt("Mesh distortion at step %d (stroke %.3f mm): %s. Automatic cutbacks, remeshing and local refinement could not recover.",
+                                                   step_index, gap0 - gap, why.c_str()));
+        if (P.auto_step) {
+            double used = P.ram * dt;
+            ds_cur = used_cutback > 0 ? rmax(used, step_cap / (1 << P.max_cutbacks)) : rmin(step_cap, 1.5 * ds_cur);
+        }
+        View3 V = view();
+        k_strain_damage<<<grid(topo.ne), 256, 0, st>>>(V, dt);
+        warm = 1;
+        iterations = its;
+        last_cutbacks = used_cutback;
+        last_dt = dt;
+        double vol = volume();
+        if (info) {
+            info->step = step_index;
+            info->iterations = its;
+            info->load = load;
+            info->reaction = reaction;
+            info->stroke = gap0 - gap;
+            info->gap = gap;
+            info->time = time;
+            info->dt = dt;
+            info->volume_change_pct = 100.0 * (vol - vol0) / vol0;
+            info->last_rel = last_rel;
+            info->n_factor = n_fact;
+            info->n_pcg = n_pcg;
+            info->remesh_requests = remesh_requests;
+            info->cutbacks = used_cutback;
+        }
+    }
+
+    // ---------------------------------------------------------------- array access
+    struct ArrRef {
+        void *p;
+        size_t count;
+        int bytes;
+    };
+    ArrRef array(const std::string &nm)
+    {
+        size_t nn = topo.nn, ne = topo.ne, nd = topo.ndof;
+#define A(name, buf, cnt) if (nm == name) return ArrRef{(void *)(buf).p, (size_t)(cnt), (int)sizeof(*(buf).p)};
+        A("x", d_x, 3 * nn) A("vg", d_vg, 3 * nn) A("v", d_vbuf[vcur], nd) A("r", d_r, nd) A("dv", d_dv, nd) A("b", d_b, nd)
+        A("eps", d_eps, ne) A("dmg", d_dmg, ne) A("el_sig", d_elsig, ne) A("el_rate", d_elrate, ne)
+        A("el_mean", d_elmean, ne) A("el_dev", d_eldev, 6 * ne) A("grad", d_grad, 12 * ne) A("vol", d_vol, ne)
+        A("ax", d_ax, 9 * nn) A("fixed_val", d_fixedval, nd) A("k_fric", d_kfric, nn) A("a_fric", d_afric, nn)
+        A("v_node", d_vnode, nn) A("kvol", d_kvol, topo.nnz) A("val", d_val, topo.nnz) A("h_local", d_hloc, nn)
+        A("contact", d_contact, nn) A("release", d_release, nn) A("fixed", d_fixed, nd) A("n_fix", d_nfix, nn)
+        A("die_axis", d_dieaxis, nn) A("nbr_start", d_nbr_start, nn + 1) A("nbr", d_nbr, topo.nbr.size())
+        A("e_r", d_er, 12 * ne) A("g_coef", d_gcoef, 3 * topo.g_node.size()) A("g_node", d_gnode, topo.g_node.size())
+        A("g_start", d_gstart, nn + 1) A("vg_prev", d_vgprev, 3 * nn)
+#undef A
+        if (nm == "e_nbr") return ArrRef{(void *)topo.e_nbr.data(), topo.e_nbr.size(), -4};
+        if (nm == "bface") return ArrRef{(void *)topo.bface.data(), topo.bface.size(), -4};
+        if (nm == "is_surface") return ArrRef{(void *)topo.is_surface.data(), topo.is_surface.size(), -1};
+        throw Failure(IFEA_INPUT_INVALID, "unknown array name '" + nm + "'");
+    }
+
+    double scalar(const std::string &nm)
+    {
+#define S(name, v) if (nm == name) return (double)(v);
+        S("gap", gap) S("gap0", gap0) S("time", time) S("load", load) S("reaction", reaction) S("power", power)
+        S("iterations", iterations) S("last_rel", last_rel) S("vol0", vol0) S("step_index", step_index)
+        S("n_pcg", n_pcg) S("n_fact", n_fact) S("n_newton", n_newton) S("n_assemble", n_assemble)
+        S("remesh_requests", remesh_requests) S("projection_reverts", projection_reverts)
+        S("corner_penetrations", corner_penetrations) S("rate_ref", rate_ref) S("rate_cut", rate_cut)
+        S("sig_ref", sig_ref) S("k_pen", k_pen) S("u0", u0) S("nnz", topo.nnz) S("ds_cur", ds_cur) S("warm", warm)
+        S("rnorm", rnorm) S("beta", beta_last) S("max_diag", max_diag) S("have_factor", have_factor)
+        S("pcg_skip", pcg_skip) S("pcg_failures", pcg_failures) S("lin_its", lin_its) S("nbf", topo.bowner.size())
+        S("recovery_pass", recovery_pass) S("factor_nnz", lin->factor_nonzeros()) S("max_nbr", topo.max_nbr)
+        S("nn", topo.nn) S("ne", topo.ne) S("ndof", topo.ndof) S("last_dt", last_dt)
+#undef S
+        if (nm == "volume") return volume();
+        if (nm == "min_quality") return min_quality(d_x);
+        throw Failure(IFEA_INPUT_INVALID, "unknown scalar name '" + nm + "'");
+    }
+    void set_scalar(const std::string &nm, double v)
+    {
+        if (nm == "gap") gap = v;
+        else if (nm == "recovery_pass") recovery_pass = (int)v;
+        else if (nm == "ds_cur") ds_cur = v;
+        else if (nm == "warm") warm = (int)v;
+        else throw Failure(IFEA_INPUT_INVALID, "unknown scalar name '" + nm + "'");
+    }
+};
+
+}  // namespace ifea
+
+using ifea::Failure;
+using ifea::Forging3D;
+
+struct ifea3d {
+    Forging3D *s;
+};
+
+template <typename F>
+static ifea_status guarded(ifea3d *c, F &&f)
+{
+    if (!c || !c->s) return IFEA_INPUT_INVALID;
+    try {
+        f(*c->s);
+        c->s->err.clear();
+        return IFEA_OK;
+    } catch (Failure &e) {
+        c->s->err = e.what();
+        return e.status;
+    } catch (std::bad_alloc &) {
+        c->s->err = "host out of memory";
+        return IFEA_CUDA_ERROR;
+    } catch (std::exception &e) {
+        c->s->err = e.what();
+        return IFEA_CUDA_ERROR;
+    }
+}
+
+extern "C" {
+
+ifea_status ifea3d_create(const ifea3d_params *params, ifea3d **out)
+{
+    if (!params || !out) return IFEA_INPUT_INVALID;
+    *out = nullptr;
+    if (!(params->ram > 0) || !(params->h > 0) || !(params->ds > 0) || !(params->size > 0) || params->max_iter < 1 ||
+        params->sym_factor < 1)
+        return IFEA_INPUT_INVALID;
+    try {
+        ifea3d *c = new ifea3d;
+        c->s = new Forging3D(*params);
+        *out = c;
+        return IFEA_OK;
+    } catch (Failure &e) {
+        return e.status;
+    } catch (...) {
+        return IFEA_CUDA_ERROR;
+    }
+}
+
+void ifea3d_destroy(ifea3d *ctx)
+{
+    if (!ctx) return;
+    delete ctx->s;
+    delete ctx;
+}
+
+const char *ifea3d_last_error(const ifea3d *ctx) { return ctx && ctx->s ? ctx->s->err.c_str() : "null context"; }
+
+ifea_status ifea3d_set_mesh(ifea3d *ctx, int32_t nn, int32_t ne, const double *x, const int32_t *tets,
+                            const uint8_t *on_x0, const uint8_t *on_y0)
+{
+    if (!x || !tets || !on_x0 || !on_y0) return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) { s.set_mesh(nn, ne, x, tets, on_x0, on_y0); });
+}
+
+ifea_status ifea3d_set_die(ifea3d *ctx, int32_t side, int32_t nx, int32_t ny, double x0, double y0, double dx, const double *h)
+{
+    if (!h) return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) { s.set_die(side, nx, ny, x0, y0, dx, h); });
+}
+
+ifea_status ifea3d_init(ifea3d *ctx, double gap0, double min_x, double min_y, double min_z, double max_x, double max_y)
+{
+    return guarded(ctx, [&](Forging3D &s) { s.init(gap0, min_x, min_y, min_z, max_x, max_y); });
+}
+
+ifea_status ifea3d_step(ifea3d *ctx, ifea_step_info *info, const volatile int32_t *cancel)
+{
+    return guarded(ctx, [&](Forging3D &s) { s.step(info, cancel); });
+}
+
+ifea_status ifea3d_pattern_size(ifea3d *ctx, int64_t *nnz, int32_t *ndof)
+{
+    return guarded(ctx, [&](Forging3D &s) {
+        if (nnz) *nnz = s.topo.nnz;
+        if (ndof) *ndof = s.topo.ndof;
+    });
+}
+
+ifea_status ifea3d_get_pattern(ifea3d *ctx, int32_t *col_ptr, int32_t *row_idx)
+{
+    return guarded(ctx, [&](Forging3D &s) {
+        if (col_ptr) memcpy(col_ptr, s.topo.col_ptr.data(), s.topo.col_ptr.size() * sizeof(int32_t));
+        if (row_idx) memcpy(row_idx, s.topo.row_idx.data(), s.topo.row_idx.size() * sizeof(int32_t));
+    });
+}
+
+ifea_status ifea3d_prepare_step(ifea3d *ctx)
+{
+    return guarded(ctx, [&](Forging3D &s) { s.prepare_step(); });
+}
+
+ifea_status ifea3d_assemble(ifea3d *ctx, int32_t matrix, int32_t newton, const double *v_host, double *energy, double *power)
+{
+    return guarded(ctx, [&](Forging3D &s) {
+        const double *v = s.d_vbuf[s.vcur];
+        if (v_host) {
+            s.d_vbuf[1 - s.vcur].upload(v_host, s.topo.ndof, s.st);
+            v = s.d_vbuf[1 - s.vcur];
+        }
+        double e = s.assemble(matrix ? ifea::ASM_MATRIX : ifea::ASM_RESIDUAL, newton, v, false, power);
+        if (energy) *energy = e;
+    });
+}
+
+ifea_status ifea3d_apply_bc(ifea3d *ctx, double *max_diag)
+{
+    return guarded(ctx, [&](Forging3D &s) {
+        s.apply_bc_separately();
+        if (max_diag) *max_diag = s.max_diag;
+    });
+}
+
+ifea_status ifea3d_solve_velocity(ifea3d *ctx, int32_t *iterations, int32_t *converged, const volatile int32_t *cancel)
+{
+    return guarded(ctx, [&](Forging3D &s) {
+        bool conv = false;
+        int it = s.solve_velocity(&conv, cancel);
+        if (iterations) *iterations = it;
+        if (converged) *converged = conv;
+    });
+}
+
+ifea_status ifea3d_final_evaluation(ifea3d *ctx, double *power, double *reaction)
+{
+    return guarded(ctx, [&](Forging3D &s) {
+        double p = s.final_evaluation(reaction);
+        if (power) *power = p;
+    });
+}
+
+ifea_status ifea3d_try_update(ifea3d *ctx, double dt, int32_t *ok)
+{
+    return guarded(ctx, [&](Forging3D &s) {
+        std::string why;
+        bool r = s.try_update(dt, why);
+        if (ok) *ok = r;
+        s.err = why;
+    });
+}
+
+ifea_status ifea3d_set_stream(ifea3d *ctx, void *cuda_stream)
+{
+    return guarded(ctx, [&](Forging3D &s) { s.set_stream((cudaStream_t)cuda_stream); });
+}
+
+ifea_status ifea3d_set_warm(ifea3d *ctx, int32_t warm)
+{
+    return guarded(ctx, [&](Forging3D &s) { s.warm = warm; });
+}
+
+ifea_status ifea3d_array_size(ifea3d *ctx, const char *name, int64_t *count, int32_t *elem_bytes)
+{
+    if (!name) return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) {
+        auto a = s.array(name);
+        if (count) *count = (int64_t)a.count;
+        if (elem_bytes) *elem_bytes = a.bytes < 0 ? -a.bytes : a.bytes;
+    });
+}
+
+ifea_status ifea3d_get_array(ifea3d *ctx, const char *name, void *dst, int64_t count)
+{
+    if (!name || !dst) return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) {
+        auto a = s.array(name);
+        if ((size_t)count != a.count) throw Failure(IFEA_INPUT_INVALID, "array size mismatch for '" + std::string(name) + "'");
+        if (a.bytes < 0) {
+            memcpy(dst, a.p, a.count * (size_t)(-a.bytes));
+            return;
+        }
+        ifea::cuda_check(cudaMemcpyAsync(dst, a.p, a.count * (size_t)a.bytes, cudaMemcpyDeviceToHost, s.st), "D2H array");
+        ifea::cuda_check(cudaStreamSynchronize(s.st), "cudaStreamSynchronize");
+    });
+}
+
+ifea_status ifea3d_set_array(ifea3d *ctx, const char *name, const void *src, int64_t count)
+{
+    if (!name || !src) return IFEA_INPUT_INVALID;
+    std::string nm(name);
+    if (nm != "x" && nm != "vg" && nm != "eps" && nm != "el_sig" && nm != "contact" && nm != "v" && nm != "dmg" &&
+        nm != "el_rate" && nm != "el_mean" && nm != "el_dev")
+        return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) {
+        auto a = s.array(nm);
+        if ((size_t)count != a.count || a.bytes < 0) throw Failure(IFEA_INPUT_INVALID, "array size mismatch for '" + nm + "'");
+        ifea::cuda_check(cudaMemcpyAsync(a.p, src, a.count * (size_t)a.bytes, cudaMemcpyHostToDevice, s.st), "H2D array");
+        ifea::cuda_check(cudaStreamSynchronize(s.st), "cudaStreamSynchronize");
+    });
+}
+
+ifea_status ifea3d_get_scalar(ifea3d *ctx, const char *name, double *value)
+{
+    if (!name || !value) return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) { *value = s.scalar(name); });
+}
+
+ifea_status ifea3d_set_scalar(ifea3d *ctx, const char *name, double value)
+{
+    if (!name) return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) { s.set_scalar(name, value); });
+}
+
+}  // extern "C"

@@ -1,0 +1,197 @@
+/*
+ * ifea_gpu.h — C ABI of the B200 (sm_100a) forging hot path.
+ *
+ * The per-Newton-iteration path of ImpressionFEA.Core's rigid-viscoplastic forging solvers runs on the GPU:
+ * element stiffness and residual (linear tets with averaged-nodal-pressure penalty; 4-node axisymmetric /
+ * plane-strain quads with reduced-integration penalty), rigid-die contact frames and m*k friction, deterministic
+ * gather-assembly into the reference's fixed sparse pattern, and the Newton / line-search / PCG update around a
+ * sparse Cholesky factorisation. The host keeps the increment loop, exactly as Forging3DSolver / ForgingSolver.
+ *
+ * Conventions: plain C types only; host arrays are borrowed for the duration of the call (copied to the device);
+ * device state is owned by the context and released by *_destroy. Every call returns an ifea_status; on failure
+ * *_last_error() returns the message the reference would have put in its exception.
+ * Contexts are independent: one per solver instance, each with its own CUDA stream and library handles.
+ */
+#ifndef IFEA_GPU_H
+#define IFEA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; the mapping to the reference's exception types (Solver/SolverExceptions.cs:4-43). */
+typedef enum ifea_status {
+    IFEA_OK = 0,
+    IFEA_INPUT_INVALID = 1,     /* InputValidationException                         */
+    IFEA_DIVERGED = 2,          /* SolverDivergenceException                        */
+    IFEA_MESH_DISTORTED = 3,    /* MeshDistortionException                          */
+    IFEA_NOT_SPD = 4,           /* MatrixNotPositiveDefiniteException               */
+    IFEA_BAD_STATE = 5,         /* InvalidOperationException (e.g. stepping after closure) */
+    IFEA_CUDA_ERROR = 6,        /* EngineUnavailableException (device or library failure) */
+    IFEA_CANCELLED = 7          /* OperationCanceledException                       */
+} ifea_status;
+
+/* NodeContact (Simulation/SimulationResult.cs:17-22). */
+enum { IFEA_FREE = 0, IFEA_BOTTOM_DIE = 1, IFEA_TOP_DIE = 2 };
+
+/* ------------------------------------------------------------------ 3D (Forging3DSolver) */
+
+/* SimulationConfig3D fields and the Forging3DSolver statics the path reads
+ * (ThreeD/SimulationConfig3D.cs:19-76; ThreeD/Forging3DSolver.cs:27-50, :1048). */
+typedef struct ifea3d_params {
+    double C, N, M, eps0;         /* FlowStressLaw (Materials/FlowStressLaw.cs:6)          */
+    double friction;              /* FrictionFactor m                                      */
+    double ram;                   /* RamSpeed, mm/s                                        */
+    double h;                     /* ElementSize, mm                                       */
+    double ds;                    /* StrokeIncrement, mm                                   */
+    double tol;                   /* Tolerance on |dv|/|v|                                 */
+    int32_t max_iter;             /* MaxIterations                                         */
+    int32_t auto_step;            /* AutoStep                                              */
+    int32_t max_cutbacks;         /* MaxCutbacks                                           */
+    double remesh_quality;        /* RemeshQuality                                         */
+    double size;                  /* rateRef = ram / size (Forging3DSolver.cs:145-146)     */
+    int32_t sym_x, sym_y, sym_factor;
+    double penalty_factor;        /* PenaltyFactor (1e4)                                   */
+    double newton_blend;          /* NewtonBlend (0.6)                                     */
+    int32_t quadratic_ls;         /* QuadraticLineSearch                                   */
+    int32_t extrapolate_start;    /* ExtrapolateStart                                      */
+    int32_t adaptive_newton;      /* AdaptiveNewton                                        */
+    int32_t sticky_secant;        /* StickySecant                                          */
+    int32_t pcg_budget;           /* PcgBudget (15)                                        */
+} ifea3d_params;
+
+/* Per-increment telemetry (ForgingSnapshot fields the solver fills, Simulation/SimulationResult.cs:25-84). */
+typedef struct ifea_step_info {
+    int32_t step;                 /* StepIndex                                             */
+    int32_t iterations;           /* Newton iterations of the accepted pass                */
+    double load;                  /* LoadNewton = power / ram * symmetry factor            */
+    double reaction;              /* top-die reaction, symmetry-scaled                     */
+    double stroke;                /* gap0 - gap                                            */
+    double gap;                   /* remaining die gap                                     */
+    double time;                  /* process time                                          */
+    double dt;                    /* time increment used                                   */
+    double volume_change_pct;     /* VolumeChangePercent                                   */
+    double last_rel;              /* |dv|/|v| of the last iteration                        */
+    int32_t n_factor;             /* factorisations so far                                 */
+    int32_t n_pcg;                /* PCG solves so far                                     */
+    int32_t remesh_requests;      /* increments where the reference would have remeshed    */
+    int32_t cutbacks;             /* cutbacks used in this increment                       */
+} ifea_step_info;
+
+typedef struct ifea3d ifea3d;
+
+/* new Forging3DSolver(config) minus the internal mesher (Forging3DSolver.cs:125-187). */
+ifea_status ifea3d_create(const ifea3d_params *params, ifea3d **out);
+void ifea3d_destroy(ifea3d *ctx);
+const char *ifea3d_last_error(const ifea3d *ctx);
+
+/* Mesh handed over by the host mesher (IsosurfaceStuffing result, Forging3DSolver.cs:153-155 / BuildMesh :205-206):
+ * x = nn*3 coordinates, tets = ne*4 positively oriented node ids, symmetry-plane flags per node.
+ * Builds TetMesh topology, the two-ring pattern (BuildPattern :469-521) and the slot maps (:1248-1261). */
+ifea_status ifea3d_set_mesh(ifea3d *ctx, int32_t nn, int32_t ne, const double *x, const int32_t *tets,
+                            const uint8_t *on_x0, const uint8_t *on_y0);
+
+/* Height-field die (ThreeD/HeightFieldDie.cs:15-26): side 0 = bottom, 1 = top (closed position);
+ * samples h[(ny+1)*(nx+1)], row-major in y. */
+ifea_status ifea3d_set_die(ifea3d *ctx, int32_t side, int32_t nx, int32_t ny, double x0, double y0, double dx,
+                           const double *h);
+
+/* Constructor tail (Forging3DSolver.cs:156-184): initial gap, initial contact and placement, initial velocity
+ * from the billet bounds (min_x, min_y, min_z, max_x, max_y), reference volume. */
+ifea_status ifea3d_init(ifea3d *ctx, double gap0, double min_x, double min_y, double min_z, double max_x,
+                        double max_y);
+
+/* One increment: Forging3DSolver.Step (:540-638). Remeshing is host-side and out of this library's scope;
+ * where the reference would remesh, the increment continues as if the remesh had been rejected and the
+ * request is counted in info->remesh_requests. cancel (may be NULL) is polled between Newton iterations. */
+ifea_status ifea3d_step(ifea3d *ctx, ifea_step_info *info, const volatile int32_t *cancel);
+
+/* Pattern of the assembled system: full symmetric CSC in 3x3 node blocks (BuildPattern :496-515). */
+ifea_status ifea3d_pattern_size(ifea3d *ctx, int64_t *nnz, int32_t *ndof);
+ifea_status ifea3d_get_pattern(ifea3d *ctx, int32_t *col_ptr, int32_t *row_idx);
+
+/* Lower-level steps of one increment, for teacher-forced parity (each mirrors a private method). */
+ifea_status ifea3d_prepare_step(ifea3d *ctx);                                       /* PrepareStep :660-758   */
+ifea_status ifea3d_assemble(ifea3d *ctx, int32_t matrix, int32_t newton, const double *v_host,
+                            double *energy, double *power);                         /* Assemble :1115-1217    */
+ifea_status ifea3d_apply_bc(ifea3d *ctx, double *max_diag);                         /* SolveVelocity :892-913 */
+ifea_status ifea3d_solve_velocity(ifea3d *ctx, int32_t *iterations, int32_t *converged,
+                                  const volatile int32_t *cancel);                  /* SolveVelocity :875-948 */
+ifea_status ifea3d_final_evaluation(ifea3d *ctx, double *power, double *reaction); /* FinalEvaluation        */
+ifea_status ifea3d_try_update(ifea3d *ctx, double dt, int32_t *ok);                 /* TryUpdate :1455-1537   */
+ifea_status ifea3d_set_warm(ifea3d *ctx, int32_t warm);
+/* Issue all further work of this context on the caller's CUDA stream (a cudaStream_t; the caller keeps it alive
+ * for the context's lifetime). Lets a host time the context with events on its own stream. */
+ifea_status ifea3d_set_stream(ifea3d *ctx, void *cuda_stream);
+
+/* Copy a named state array to host memory (count elements of the named array's type):
+ * "x","vg","v","r","dv" (double), "eps","dmg","el_sig","el_rate","el_mean","el_dev","grad","vol","ax",
+ * "fixed_val","k_fric","a_fric","v_node","kvol","val","h_local" (double), "contact","release","fixed"
+ * (uint8), "n_fix","die_axis","e_nbr","nbr_start","nbr" (int32). Returns IFEA_INPUT_INVALID on unknown names. */
+ifea_status ifea3d_get_array(ifea3d *ctx, const char *name, void *dst, int64_t count);
+ifea_status ifea3d_array_size(ifea3d *ctx, const char *name, int64_t *count, int32_t *elem_bytes);
+/* Replace a named state array ("x","vg","eps","el_sig","contact","v","dmg") with host data. */
+ifea_status ifea3d_set_array(ifea3d *ctx, const char *name, const void *src, int64_t count);
+ifea_status ifea3d_get_scalar(ifea3d *ctx, const char *name, double *value);
+ifea_status ifea3d_set_scalar(ifea3d *ctx, const char *name, double value);
+
+/* ------------------------------------------------------------------ ISpdSolver (Solver/Linear/ISpdSolver.cs:24-41)
+ * Sparse SPD direct solver over a full symmetric CSC pattern, for the reference's pluggable factorisation seam
+ * (replaces CudssSolver.cs:105-145 behind ISpdSolver). Host buffers, like the reference's backends. */
+typedef struct ifea_spd ifea_spd;
+ifea_status ifea_spd_create(ifea_spd **out);
+void ifea_spd_destroy(ifea_spd *s);
+const char *ifea_spd_last_error(const ifea_spd *s);
+ifea_status ifea_spd_analyze(ifea_spd *s, int32_t n, const int32_t *col_ptr, const int32_t *row_idx);
+ifea_status ifea_spd_factorize(ifea_spd *s, const double *values);
+ifea_status ifea_spd_solve(ifea_spd *s, const double *b, double *x);
+int64_t ifea_spd_factor_nonzeros(const ifea_spd *s);
+const char *ifea_spd_name(const ifea_spd *s);
+
+/* ------------------------------------------------------------------ 2D (ForgingSolver) */
+
+/* SimulationConfig + DieSet fields the 2D path reads (Simulation/SimulationConfig.cs:14-45, Geometry/DieSet.cs). */
+typedef struct ifea2d_params {
+    double C, N, M, eps0;
+    double friction;
+    double ram;
+    double ds;                    /* StrokeIncrement                                       */
+    double tol;
+    int32_t max_iter;
+    int32_t axisymmetric;         /* Symmetry.Axisymmetric (1) / PlaneStrain (0)           */
+    double length;                /* BilletLength (plane strain)                           */
+    double radius, height;        /* billet                                                */
+    int32_t nx, nz;               /* ElementsX, ElementsZ                                  */
+} ifea2d_params;
+
+typedef struct ifea2d ifea2d;
+/* new ForgingSolver(config) (Solver/ForgingSolver.cs:104-145): structured mesh, RCM numbering, dies as
+ * piecewise-linear profiles (x strictly increasing, closed position). */
+ifea_status ifea2d_create(const ifea2d_params *params, int32_t n_bottom, const double *bottom_xy, int32_t n_top,
+                          const double *top_xy, ifea2d **out);
+void ifea2d_destroy(ifea2d *ctx);
+const char *ifea2d_last_error(const ifea2d *ctx);
+ifea_status ifea2d_step(ifea2d *ctx, ifea_step_info *info, const volatile int32_t *cancel); /* Advance :215-290 */
+ifea_status ifea2d_prepare(ifea2d *ctx);                      /* PrepareConstraints + LoadVelocityGuess */
+ifea_status ifea2d_assemble(ifea2d *ctx, int32_t matrix, int32_t newton, const double *v_host, double *energy,
+                            double *power);                   /* Assemble :471-538 */
+ifea_status ifea2d_solve_velocity(ifea2d *ctx, int32_t picard_fallback, int32_t *iterations, int32_t *converged);
+ifea_status ifea2d_get_array(ifea2d *ctx, const char *name, void *dst, int64_t count);
+ifea_status ifea2d_array_size(ifea2d *ctx, const char *name, int64_t *count, int32_t *elem_bytes);
+ifea_status ifea2d_get_scalar(ifea2d *ctx, const char *name, double *value);
+
+/* SymmetricBandMatrix (Solver/SymmetricBandMatrix.cs:7-111) factorised on the GPU: lower band stored row-wise,
+ * a[i*(b+1) + (j-i+b)]. Host buffers. On a non-positive pivot returns IFEA_NOT_SPD with *bad_row = the row. */
+ifea_status ifea_band_factor_solve(int32_t n, int32_t half_bandwidth, double *band, double *rhs, int32_t *bad_row,
+                                   double *pivot);
+
+/* Library build / device description for the log. */
+const char *ifea_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
