@@ -17,6 +17,7 @@ from oracle import Oracle3D
 pytestmark = pytest.mark.gpu
 
 RTOL_ELEM = 1e-12      # per-element / per-node FP64 arithmetic (a few ulps of pow())
+RTOL_ENERGY = 1e-10    # global sums: 1/2 v.K_vol.v cancels the penalty terms, so its summation order shows
 RTOL_STATE = 1e-6      # velocity, strain and load over Newton iterations and increments
 
 
@@ -86,7 +87,7 @@ def test_assemble_matrix_residual_energy(pair, newton):
     v = ora.array("v") * (1 + 0.01 * np.sin(np.arange(len(ora.array("v")))))  # a non-trivial velocity field
     eg, pg = gpu.assemble(1, newton, v)
     eo, po = ora.assemble(1, newton, v)
-    assert abs(eg / eo - 1) < 1e-12 and abs(pg / po - 1) < 1e-12
+    assert abs(eg / eo - 1) < RTOL_ENERGY and abs(pg / po - 1) < RTOL_ENERGY
     _close(gpu.array("val"), ora.array("val"), RTOL_ELEM, "assembled values")
     _close(gpu.array("r"), ora.array("r"), 1e-11, "residual")
     _close(gpu.array("el_sig"), ora.array("el_sig"), RTOL_ELEM, "element flow stress")
@@ -104,7 +105,7 @@ def test_residual_only_assembly(pair):
     v = ora.array("v")
     eg, pg = gpu.assemble(0, 0, v)
     eo, po = ora.assemble(0, 0, v)
-    assert abs(eg / eo - 1) < 1e-12 and abs(pg / po - 1) < 1e-12
+    assert abs(eg / eo - 1) < RTOL_ENERGY and abs(pg / po - 1) < RTOL_ENERGY
     _close(gpu.array("r"), ora.array("r"), 1e-11, "residual")
 
 
