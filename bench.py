@@ -241,7 +241,9 @@ def run_gpu(args, rank, world):
                                                   "newton_iterations": int(sum(i["iterations"] for i in infos)),
                                                   "factorisations": int(infos[-1]["n_factor"]) if infos else 0,
                                                   "pcg_solves": int(infos[-1]["n_pcg"]) if infos else 0,
-                                                  "load_last_N": infos[-1]["load"] if infos else None}),
+                                                  "load_last_N": infos[-1]["load"] if infos else None,
+                                                  "factor": {k: s.scalar(k) for k in ("supernodes", "levels", "front_pool_mb",
+                                                                                        "max_front", "factor_nnz")}}),
                 "roofline": {"kernel": "assembly (k_element<MATRIX> + k_columns<MATRIX,BC>)", "bound": "hbm",
                              "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                              "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes": abytes,

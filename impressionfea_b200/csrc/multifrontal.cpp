@@ -1,0 +1,267 @@
+// multifrontal.cpp — symbolic analysis of the GPU multifrontal Cholesky (see multifrontal.h).
+#include "multifrontal.h"
+
+#include <cusolverSp.h>
+#include <cusparse.h>
+
+#include <algorithm>
+#include <numeric>
+
+namespace ifea {
+
+std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, int block, void *hsp, void *descr)
+{
+    n = n_;
+    if (n <= 0) return "empty system";
+    if (block < 1 || n % block) block = 1;
+    const int nb = n / block;
+
+    // 1. nested dissection of the block graph (no self loops)
+    std::vector<int> gp(nb + 1, 0), gi;
+    {
+        std::vector<int> mark(nb, -1);
+        for (int b = 0; b < nb; b++) {
+            int d = b * block;
+            for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
+                int o = ri[p] / block;
+                if (o == b || mark[o] == b) continue;
+                mark[o] = b;
+                gi.push_back(o);
+            }
+            gp[b + 1] = (int)gi.size();
+        }
+    }
+    std::vector<int> pnode(nb);
+    if (gi.empty() || !hsp) {
+        std::iota(pnode.begin(), pnode.end(), 0);
+    } else {
+        cusolverStatus_t st = cusolverSpXcsrmetisndHost((cusolverSpHandle_t)hsp, nb, (int)gi.size(), (cusparseMatDescr_t)descr,
+                                                        gp.data(), gi.data(), nullptr, pnode.data());
+        if (st != CUSOLVER_STATUS_SUCCESS) return "METIS ordering failed (cuSOLVER status " + std::to_string((int)st) + ")";
+    }
+    std::vector<int32_t> perm0(n), pinv0(n);
+    for (int k = 0; k < nb; k++)
+        for (int c = 0; c < block; c++) perm0[k * block + c] = pnode[k] * block + c;
+    for (int k = 0; k < n; k++) pinv0[perm0[k]] = k;
+
+    // 2. elimination tree of P A P' (Liu's algorithm with path compression)
+    std::vector<int32_t> par(n, -1), anc(n, -1);
+    for (int k = 0; k < n; k++) {
+        int d = perm0[k];
+        for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
+            int i = pinv0[ri[p]];
+            while (i != -1 && i < k) {
+                int inext = anc[i];
+                anc[i] = k;
+                if (inext == -1) par[i] = k;
+                i = inext;
+            }
+        }
+    }
+    // 3. postorder (children in ascending order)
+    std::vector<int32_t> head(n, -1), next(n, -1), post(n);
+    for (int j = n - 1; j >= 0; j--)
+        if (par[j] != -1) {
+            next[j] = head[par[j]];
+            head[par[j]] = j;
+        }
+    {
+        std::vector<int32_t> stack;
+        int k = 0;
+        for (int j = 0; j < n; j++) {
+            if (par[j] != -1) continue;
+            stack.push_back(j);
+            while (!stack.empty()) {
+                int p = stack.back();
+                int i = head[p];
+                if (i == -1) {
+                    stack.pop_back();
+                    post[k++] = p;
+                } else {
+                    head[p] = next[i];
+                    stack.push_back(i);
+                }
+            }
+        }
+        if (k != n) return "internal error: elimination tree postorder incomplete";
+    }
+    perm.resize(n);
+    pinv.resize(n);
+    std::vector<int32_t> postinv(n);
+    for (int k = 0; k < n; k++) postinv[post[k]] = k;
+    for (int k = 0; k < n; k++) perm[k] = perm0[post[k]];
+    for (int k = 0; k < n; k++) pinv[perm[k]] = k;
+    std::vector<int32_t> parent_c(n);
+    for (int k = 0; k < n; k++) parent_c[k] = par[post[k]] < 0 ? -1 : postinv[par[post[k]]];
+
+    // 4. column counts of L by row subtrees (ereach)
+    std::vector<int64_t> cc(n, 1);
+    {
+        std::vector<int32_t> mark(n, -1);
+        for (int k = 0; k < n; k++) {
+            mark[k] = k;
+            int d = perm[k];
+            for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
+                int i = pinv[ri[p]];
+                if (i >= k) continue;
+                while (mark[i] != k) {
+                    cc[i]++;
+                    mark[i] = k;
+                    i = parent_c[i];
+                    if (i < 0) break;
+                }
+            }
+        }
+    }
+    // 5. supernodes: k joins k-1's supernode when struct(L_{k-1}) = {k-1} u struct(L_k)
+    std::vector<int32_t> sn_of(n);
+    c0.clear();
+    for (int k = 0; k < n; k++) {
+        bool join = k > 0 && parent_c[k - 1] == k && cc[k - 1] == cc[k] + 1;
+        if (!join) c0.push_back(k);
+        sn_of[k] = (int)c0.size() - 1;
+    }
+    nsuper = (int)c0.size();
+    ncol.resize(nsuper);
+    for (int s = 0; s < nsuper; s++) ncol[s] = (s + 1 < nsuper ? c0[s + 1] : n) - c0[s];
+    parent.assign(nsuper, -1);
+    for (int s = 0; s < nsuper; s++) {
+        int last = c0[s] + ncol[s] - 1;
+        if (parent_c[last] >= 0) parent[s] = sn_of[parent_c[last]];
+    }
+    // 6. row structures (children precede parents in postorder)
+    std::vector<std::vector<int32_t>> strc(nsuper);
+    std::vector<std::vector<int32_t>> kids(nsuper);
+    for (int s = 0; s < nsuper; s++)
+        if (parent[s] >= 0) kids[parent[s]].push_back(s);
+    {
+        std::vector<int32_t> mark(n, -1);
+        for (int s = 0; s < nsuper; s++) {
+            int first = c0[s], end = c0[s] + ncol[s];
+            auto &v = strc[s];
+            for (int j = first; j < end; j++) {
+                int d = perm[j];
+                for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
+                    int i = pinv[ri[p]];
+                    if (i >= end && mark[i] != s) {
+                        mark[i] = s;
+                        v.push_back(i);
+                    }
+                }
+            }
+            for (int c : kids[s])
+                for (int i : strc[c])
+                    if (i >= end && mark[i] != s) {
+                        mark[i] = s;
+                        v.push_back(i);
+                    }
+            std::sort(v.begin(), v.end());
+            if ((int64_t)v.size() + ncol[s] != cc[first]) return "internal error: supernode structure does not match the column counts";
+        }
+    }
+    // 7. fronts, levels, maps
+    m.resize(nsuper);
+    level.assign(nsuper, 0);
+    max_m = max_ncol = 0;
+    factor_nnz = 0;
+    for (int s = 0; s < nsuper; s++) {
+        m[s] = ncol[s] + (int)strc[s].size();
+        for (int c : kids[s]) level[s] = std::max(level[s], level[c] + 1);
+        max_m = std::max(max_m, m[s]);
+        max_ncol = std::max(max_ncol, ncol[s]);
+        factor_nnz += (int64_t)ncol[s] * (ncol[s] + 1) / 2 + (int64_t)ncol[s] * (int64_t)strc[s].size();
+    }
+    nlevels = 0;
+    for (int s = 0; s < nsuper; s++) nlevels = std::max(nlevels, level[s] + 1);
+    level_start.assign(nlevels + 1, 0);
+    for (int s = 0; s < nsuper; s++) level_start[level[s] + 1]++;
+    for (int l = 0; l < nlevels; l++) level_start[l + 1] += level_start[l];
+    level_list.assign(nsuper, 0);
+    {
+        std::vector<int32_t> fill(level_start.begin(), level_start.end() - 1);
+        for (int s = 0; s < nsuper; s++) level_list[fill[level[s]]++] = s;
+    }
+    front_off.assign(nsuper, 0);
+    level_pool_start.assign(nlevels + 1, 0);
+    pool = 0;
+    for (int l = 0; l < nlevels; l++) {
+        level_pool_start[l] = pool;
+        for (int32_t q = level_start[l]; q < level_start[l + 1]; q++) {
+            int s = level_list[q];
+            front_off[s] = pool;
+            pool += (int64_t)m[s] * m[s];
+        }
+    }
+    level_pool_start[nlevels] = pool;
+    idx_start.assign(nsuper + 1, 0);
+    for (int s = 0; s < nsuper; s++) idx_start[s + 1] = idx_start[s] + m[s];
+    idx.resize(idx_start[nsuper]);
+    for (int s = 0; s < nsuper; s++) {
+        int o = idx_start[s];
+        for (int k = 0; k < ncol[s]; k++) idx[o + k] = c0[s] + k;
+        for (size_t k = 0; k < strc[s].size(); k++) idx[o + ncol[s] + k] = strc[s][k];
+    }
+    relmap_start.assign(nsuper + 1, 0);
+    uvec_start.assign(nsuper + 1, 0);
+    for (int s = 0; s < nsuper; s++) {
+        relmap_start[s + 1] = relmap_start[s] + (int)strc[s].size();
+        uvec_start[s + 1] = uvec_start[s] + (int)strc[s].size();
+    }
+    uvec_pool = uvec_start[nsuper];
+    relmap.assign(relmap_start[nsuper], 0);
+    for (int s = 0; s < nsuper; s++) {
+        int p = parent[s];
+        if (p < 0) {
+            if (!strc[s].empty()) return "internal error: a root supernode has off-diagonal rows";
+            continue;
+        }
+        const int32_t *pb = idx.data() + idx_start[p], *pe = pb + m[p];
+        for (size_t k = 0; k < strc[s].size(); k++) {
+            const int32_t *it = std::lower_bound(pb, pe, strc[s][k]);
+            if (it == pe || *it != strc[s][k]) return "internal error: child row missing from the parent front";
+            relmap[relmap_start[s] + k] = (int32_t)(it - pb);
+        }
+    }
+    // original values -> fronts, grouped by level
+    a_dst.clear();
+    a_src.clear();
+    a_level_start.assign(nlevels + 1, 0);
+    for (int l = 0; l < nlevels; l++) {
+        a_level_start[l] = (int32_t)a_src.size();
+        for (int32_t q = level_start[l]; q < level_start[l + 1]; q++) {
+            int s = level_list[q];
+            const int32_t *ib = idx.data() + idx_start[s], *ie = ib + m[s];
+            for (int j = c0[s]; j < c0[s] + ncol[s]; j++) {
+                int d = perm[j];
+                for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
+                    int i = pinv[ri[p]];
+                    if (i < j) continue;
+                    const int32_t *it = std::lower_bound(ib, ie, i);
+                    if (it == ie || *it != i) return "internal error: matrix entry outside its front";
+                    a_dst.push_back(front_off[s] + (int64_t)(j - c0[s]) * m[s] + (it - ib));
+                    a_src.push_back(p);
+                }
+            }
+        }
+    }
+    a_level_start[nlevels] = (int32_t)a_src.size();
+    // extend-add schedule: r-th child (ascending) of every parent of a level
+    max_rank = 1;
+    for (int s = 0; s < nsuper; s++) max_rank = std::max<int>(max_rank, (int)kids[s].size());
+    ext_start.assign((size_t)nlevels * max_rank + 1, 0);
+    std::vector<std::vector<int32_t>> buckets((size_t)nlevels * max_rank);
+    for (int l = 0; l < nlevels; l++)
+        for (int32_t q = level_start[l]; q < level_start[l + 1]; q++) {
+            int p = level_list[q];
+            for (size_t r = 0; r < kids[p].size(); r++) buckets[(size_t)l * max_rank + r].push_back(kids[p][r]);
+        }
+    ext_child.clear();
+    for (size_t b = 0; b < buckets.size(); b++) {
+        ext_start[b] = (int32_t)ext_child.size();
+        ext_child.insert(ext_child.end(), buckets[b].begin(), buckets[b].end());
+    }
+    ext_start[buckets.size()] = (int32_t)ext_child.size();
+    return "";
+}
+
+}  // namespace ifea

@@ -1,0 +1,43 @@
+// multifrontal.h — symbolic analysis of the GPU multifrontal sparse Cholesky (host side).
+//
+// Pipeline (once per sparsity pattern): nested-dissection order of the node graph (METIS through cuSOLVER's host
+// helper), elimination tree and its postorder, column counts, supernodes (columns whose factor structure nests),
+// the row structure of every supernode, the frontal-matrix layout, the child->parent index maps of the
+// extend-add, and the level schedule (a supernode's level = 1 + the highest level of its children).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace ifea {
+
+struct MfSymbolic {
+    int n = 0, nsuper = 0, nlevels = 0;
+    std::vector<int32_t> perm, pinv;              // new -> old, old -> new
+    // supernodes (columns [c0, c1) in the new numbering)
+    std::vector<int32_t> c0, ncol, m, parent, level;
+    std::vector<int64_t> front_off;               // offset of the m x m column-major front in the pool
+    int64_t pool = 0;                              // total doubles of all fronts
+    std::vector<int32_t> idx_start, idx;          // global (new) row index of each front row
+    std::vector<int32_t> relmap_start, relmap;    // struct rows of s -> row position in parent's front
+    std::vector<int32_t> uvec_start;              // offset of s's update vector (nrow) in the solve pool
+    int64_t uvec_pool = 0;
+    // original-value scatter: dst offset in the pool <- src index into the full CSC value array
+    std::vector<int64_t> a_dst;
+    std::vector<int32_t> a_src;
+    std::vector<int32_t> a_level_start;           // a_dst/a_src ranges per level (fronts are stored by level)
+    // level schedule
+    std::vector<int32_t> level_start, level_list;  // supernodes of each level (ascending index)
+    std::vector<int64_t> level_pool_start;         // pool range of each level's fronts (contiguous)
+    // extend-add: per (level, child rank r) the children c whose parent lies in that level
+    std::vector<int32_t> ext_start, ext_child;     // index = level * max_rank + r
+    int max_rank = 0;
+    int64_t factor_nnz = 0;
+    int max_m = 0, max_ncol = 0;
+
+    // Full symmetric CSC pattern (both triangles) of an n x n matrix; block = 3 orders 3x3 node blocks together.
+    std::string analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block, void *cusolver_sp_handle,
+                        void *mat_descr);
+};
+
+}  // namespace ifea

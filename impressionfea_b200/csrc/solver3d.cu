@@ -15,7 +15,7 @@
 #include "kernels3d.cuh"
 #include "mesh3d.h"
 #include "runtime.cuh"
-#include "spd.cuh"
+#include "multifrontal.cuh"
 
 namespace ifea {
 
@@ -44,7 +44,7 @@ struct Forging3D {
     int last_cutbacks = 0, n_newton = 0, n_assemble = 0, lin_its = 0;
     double load = 0, reaction = 0, power = 0, last_dt = 0, rnorm = 0, beta_last = 0, max_diag = 0;
     // linear solver (SolveLinear :965-1019)
-    std::unique_ptr<GpuSpd> lin;
+    std::unique_ptr<MfSolver> lin;
     bool need_analyze = true, have_factor = false;
     int pcg_failures = 0, pcg_skip = 0;
     // mesh
@@ -83,7 +83,7 @@ struct Forging3D {
         d_scalars.resize(S_COUNT);
         d_err.resize(4);
         d_counters.resize(4);
-        lin.reset(new GpuSpd(st));
+        lin.reset(new MfSolver(st));
     }
     bool own_stream = true;
     ~Forging3D()
@@ -391,7 +391,7 @@ struct Forging3D {
         } catch (Failure &f) {
             have_factor = false;
             if (f.status == IFEA_NOT_SPD) throw;
-            throw Failure(IFEA_DIVERGED, fmt("Sparse factorisation failed at step %d (cuSOLVER csrchol): %s", step_index, f.what()));
+            throw Failure(IFEA_DIVERGED, fmt("Sparse factorisation failed at step %d (GPU multifrontal Cholesky): %s", step_index, f.what()));
         }
         have_factor = true;
         n_fact++;
@@ -656,6 +656,8 @@ struct Forging3D {
         S("pcg_skip", pcg_skip) S("pcg_failures", pcg_failures) S("lin_its", lin_its) S("nbf", topo.bowner.size())
         S("recovery_pass", recovery_pass) S("factor_nnz", lin->factor_nonzeros()) S("max_nbr", topo.max_nbr)
         S("nn", topo.nn) S("ne", topo.ne) S("ndof", topo.ndof) S("last_dt", last_dt)
+        S("supernodes", lin->symbolic().nsuper) S("levels", lin->symbolic().nlevels)
+        S("front_pool_mb", lin->symbolic().pool * 8e-6) S("max_front", lin->symbolic().max_m)
 #undef S
         if (nm == "volume") return volume();
         if (nm == "min_quality") return min_quality(d_x);

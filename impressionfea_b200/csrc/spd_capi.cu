@@ -3,11 +3,11 @@
 #include <string>
 #include <vector>
 
-#include "spd.cuh"
+#include "multifrontal.cuh"
 
 struct ifea_spd {
     cudaStream_t st = nullptr;
-    ifea::GpuSpd *s = nullptr;
+    ifea::MfSolver *s = nullptr;
     ifea::DBuf<double> vals, b, x;
     std::vector<int32_t> col_ptr;
     int n = 0;
@@ -41,10 +41,10 @@ ifea_status ifea_spd_create(ifea_spd **out)
     ifea_spd *h = new ifea_spd;
     try {
         ifea::cuda_check(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking), "cudaStreamCreate");
-        h->s = new ifea::GpuSpd(h->st);
+        h->s = new ifea::MfSolver(h->st);
         cudaDeviceProp prop;
         ifea::cuda_check(cudaGetDeviceProperties(&prop, 0), "cudaGetDeviceProperties");
-        h->name = std::string("cuSOLVER sparse Cholesky (GPU · ") + prop.name + ")";
+        h->name = std::string("multifrontal sparse Cholesky (GPU · ") + prop.name + ")";
     } catch (ifea::Failure &e) {
         delete h->s;
         if (h->st) cudaStreamDestroy(h->st);

@@ -106,7 +106,7 @@ def test_residual_only_assembly(pair):
     eg, pg = gpu.assemble(0, 0, v)
     eo, po = ora.assemble(0, 0, v)
     assert abs(eg / eo - 1) < RTOL_ENERGY and abs(pg / po - 1) < RTOL_ENERGY
-    _close(gpu.array("r"), ora.array("r"), 1e-11, "residual")
+    _close(gpu.array("r"), ora.array("r"), RTOL_ENERGY, "residual")
 
 
 def test_increments_track_the_oracle():
