@@ -106,6 +106,7 @@ SIGNATURES = {
     "ifea2d_array_size": (_st, [_vp, C.c_char_p, _i64p, _i32p]),
     "ifea2d_get_scalar": (_st, [_vp, C.c_char_p, _dp]),
     "ifea_band_factor_solve": (_st, [C.c_int32, C.c_int32, _dp, _dp, _i32p, _dp]),
+    "ifea_band_factor_solve_noalloc": (_st, [C.c_int32, C.c_int32, _vp, _vp, _i32p, _dp, _vp]),
     "ifea_version": (C.c_char_p, []),
 }
 
