@@ -3,6 +3,7 @@
 // The control flow is Forging3DSolver's (ThreeD/Forging3DSolver.cs:540-1537): the host runs the increment
 // loop, the Newton iteration, the line search and the PCG loop, and reads back only the handful of scalars
 // those decisions need; every array operation is a device kernel on the context's stream.
+#include <chrono>
 #include <climits>
 #include <cstdarg>
 #include <cmath>
@@ -30,8 +31,19 @@ static std::string fmt(const char *f, ...)
     return buf;
 }
 
+// Adds the wall time of a scope to an accumulator (the phases end in a stream synchronisation, so host time
+// is the phase's time); the split mirrors Forging3DSolver.TimingSummary (:1924-1943).
+struct PhaseTimer {
+    double &acc;
+    std::chrono::steady_clock::time_point t0;
+    explicit PhaseTimer(double &a) : acc(a), t0(std::chrono::steady_clock::now()) {}
+    ~PhaseTimer() { acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
 struct Forging3D {
     ifea3d_params P;
+    double t_trigger = 0, t_prepare = 0, t_assemble = 0, t_linesearch = 0, t_factor = 0, t_pcg = 0, t_final = 0,
+           t_update = 0, t_total = 0;
     cudaStream_t st = nullptr;
     std::string err;
     // constants (Forging3DSolver.cs:137-150)
@@ -264,6 +276,7 @@ struct Forging3D {
     // ---------------------------------------------------------------- PrepareStep (:660-758)
     void prepare_step()
     {
+        PhaseTimer pt(t_prepare);
         View3 V = view();
         reset_err();
         k_frames<<<grid(topo.nn), 256, 0, st>>>(V);
@@ -372,7 +385,11 @@ struct Forging3D {
         if (have_factor && pcg_skip > 0) {
             pcg_skip--;
         } else if (have_factor) {
-            int its = pcg(b, x, 1e-7, P.pcg_budget);
+            int its;
+            {
+                PhaseTimer pt(t_pcg);
+                its = pcg(b, x, 1e-7, P.pcg_budget);
+            }
             if (its >= 0) {
                 pcg_failures = 0;
                 n_pcg++;
@@ -385,6 +402,7 @@ struct Forging3D {
             need_analyze = false;
         }
         try {
+            PhaseTimer pt(t_factor);
             lin->factorize(d_val);
             lin->solve(b, x);
             lin->check_finite(x);
@@ -412,7 +430,11 @@ struct Forging3D {
             if (P.sticky_secant && halved >= 2) secant_only = true;
             int newton = (warm || it > 2) && it <= newton_limit && !secant_only && !(P.adaptive_newton && halved >= 2);
             n_newton += newton;
-            double e0 = assemble(ASM_MATRIX, newton, d_vbuf[vcur], true, nullptr);
+            double e0;
+            {
+                PhaseTimer pt(t_assemble);
+                e0 = assemble(ASM_MATRIX, newton, d_vbuf[vcur], true, nullptr);
+            }
             {
                 View3 V = view();
                 k_regularise<<<grid(n), 256, 0, st>>>(V);
@@ -422,6 +444,7 @@ struct Forging3D {
             double dvdv = 0;
             double slope = -dot_read(d_b, d_dv, S_DOT, d_dv, S_NORM_B, &dvdv);
             double beta = 1;
+            PhaseTimer pls(t_linesearch);
             for (int ls = 0; ls < 8; ls++) {
                 k_axpy<<<grid(n), 256, 0, st>>>(n, d_vbuf[1 - vcur], d_vbuf[vcur], d_dv, beta);
                 double e1 = assemble(ASM_ENERGY, 0, d_vbuf[1 - vcur], false, nullptr);
@@ -447,6 +470,7 @@ struct Forging3D {
     // ---------------------------------------------------------------- FinalEvaluation (:1402-1451)
     double final_evaluation(double *reaction_out)
     {
+        PhaseTimer pt(t_final);
         double pw = 0;
         assemble(ASM_RESIDUAL, 0, d_vbuf[vcur], false, &pw);
         View3 V = view();
@@ -487,6 +511,7 @@ struct Forging3D {
 
     bool try_update(double dt, std::string &why)
     {
+        PhaseTimer pt(t_update);
         double gapT = rmax(0, gap - P.ram * dt);
         if (gapT < 1e-9) gapT = 0;
         View3 V = view();
@@ -533,15 +558,19 @@ struct Forging3D {
         if (!initialized) throw Failure(IFEA_BAD_STATE, "ifea3d_init must be called before stepping.");
         if (gap <= 1e-9) throw Failure(IFEA_BAD_STATE, "Simulation already reached the closed-die position.");
         step_index++;
+        PhaseTimer ptotal(t_total);
         // RemeshTrigger (:1867-1883): first-aid smoothing; a remesh itself is out of scope and only counted
-        double rq = P.remesh_quality;
-        if (min_quality(d_x) < rq) smooth_interior(d_x, rq, 6);
-        if (min_quality(d_x) < rq) remesh_requests++;
-        else {
-            View3 V = view();
-            k_edges_layers<<<kReduceBlocks, 256, 0, st>>>(V);
-            finalize({MAXS(S_MAXEDGE), MAXS(S_THIN)});
-            if (read_scalars()[S_MAXEDGE] > 2.8 * h) remesh_requests++;
+        {
+            PhaseTimer pt(t_trigger);
+            double rq = P.remesh_quality;
+            if (min_quality(d_x) < rq) smooth_interior(d_x, rq, 6);
+            if (min_quality(d_x) < rq) remesh_requests++;
+            else {
+                View3 V = view();
+                k_edges_layers<<<kReduceBlocks, 256, 0, st>>>(V);
+                finalize({MAXS(S_MAXEDGE), MAXS(S_THIN)});
+                if (read_scalars()[S_MAXEDGE] > 2.8 * h) remesh_requests++;
+            }
         }
         double step_cap = P.ds * h / P.h;
         int its = 0, used_cutback = 0;
@@ -656,8 +685,10 @@ struct Forging3D {
         S("pcg_skip", pcg_skip) S("pcg_failures", pcg_failures) S("lin_its", lin_its) S("nbf", topo.bowner.size())
         S("recovery_pass", recovery_pass) S("factor_nnz", lin->factor_nonzeros()) S("max_nbr", topo.max_nbr)
         S("nn", topo.nn) S("ne", topo.ne) S("ndof", topo.ndof) S("last_dt", last_dt)
+        S("t_trigger", t_trigger) S("t_prepare", t_prepare) S("t_assemble", t_assemble) S("t_linesearch", t_linesearch)
+        S("t_factor", t_factor) S("t_pcg", t_pcg) S("t_final", t_final) S("t_update", t_update) S("t_total", t_total)
         S("supernodes", lin->symbolic().nsuper) S("levels", lin->symbolic().nlevels)
-        S("front_pool_mb", lin->symbolic().pool * 8e-6) S("max_front", lin->symbolic().max_m)
+        S("front_pool_mb", lin->symbolic().pool * 8e-6) S("max_front", lin->symbolic().max_m) S("big_fronts", lin->big_fronts())
 #undef S
         if (nm == "volume") return volume();
         if (nm == "min_quality") return min_quality(d_x);
