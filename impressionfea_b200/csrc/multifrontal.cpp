@@ -159,6 +159,59 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
             if ((int64_t)v.size() + ncol[s] != cc[first]) return "internal error: supernode structure does not match the column counts";
         }
     }
+    // 6b. relaxed amalgamation: merge a supernode into its parent when it is the parent's contiguous (last) child
+    //     and the explicit zeros this adds stay small; chains inside a separator collapse into one front.
+    {
+        std::vector<int32_t> mc0(c0.begin(), c0.end()), mnc(ncol.begin(), ncol.end()), mpar(parent.begin(), parent.end());
+        std::vector<int64_t> zeros(nsuper, 0);
+        std::vector<uint8_t> alive(nsuper, 1);
+        std::vector<int32_t> rep(nsuper);  // representative (merged node) of each original supernode
+        for (int q = 0; q < nsuper; q++) rep[q] = q;
+        auto find = [&](int q) {
+            while (q >= 0 && !alive[q]) q = rep[q];
+            return q;
+        };
+        for (int p = 0; p < nsuper; p++) {
+            int c = p - 1;  // only the immediately preceding supernode can be contiguous
+            if (c < 0 || !alive[c] || find(mpar[c]) != p || mc0[c] + mnc[c] != mc0[p]) continue;
+            int64_t mp = mnc[p] + (int64_t)strc[p].size();
+            int64_t nrc = (int64_t)strc[c].size();
+            int64_t add = (int64_t)mnc[c] * (mp - nrc);                    // zeros in c's columns
+            int64_t ncm = mnc[c] + mnc[p];
+            int64_t total = ncm * (ncm + 1) / 2 + ncm * (int64_t)strc[p].size();
+            bool small = ncm <= 16;
+            if (!(small || (zeros[c] + zeros[p] + add) * 5 <= total)) continue;  // at most 20 % explicit zeros
+            // merge c into p: p keeps its parent and structure, gains c's columns and children
+            mc0[p] = mc0[c];
+            mnc[p] = (int32_t)ncm;
+            zeros[p] += zeros[c] + add;
+            alive[c] = 0;
+            rep[c] = p;
+        }
+        // compact
+        std::vector<int32_t> newid(nsuper, -1);
+        int ns = 0;
+        for (int q = 0; q < nsuper; q++)
+            if (alive[q]) newid[q] = ns++;
+        std::vector<int32_t> c0n, ncn, parn;
+        std::vector<std::vector<int32_t>> strn;
+        for (int q = 0; q < nsuper; q++) {
+            if (!alive[q]) continue;
+            c0n.push_back(mc0[q]);
+            ncn.push_back(mnc[q]);
+            int pp = find(mpar[q]);
+            parn.push_back(pp < 0 ? -1 : newid[pp]);
+            strn.push_back(std::move(strc[q]));
+        }
+        nsuper = ns;
+        c0 = c0n;
+        ncol = ncn;
+        parent = parn;
+        strc = std::move(strn);
+        kids.assign(nsuper, {});
+        for (int q = 0; q < nsuper; q++)
+            if (parent[q] >= 0) kids[parent[q]].push_back(q);
+    }
     // 7. fronts, levels, maps
     m.resize(nsuper);
     level.assign(nsuper, 0);

@@ -380,6 +380,12 @@ static __global__ void __launch_bounds__(256) k_update(Dev D, const int32_t *__r
     }
 }
 
+static __global__ void k_init_err(int *err)
+{
+    err[0] = INT_MAX;
+    err[1] = 0;
+}
+
 static __global__ void k_permute_in(int n, const int32_t *perm, const double *b, double *y)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = b[perm[i]];
@@ -501,9 +507,15 @@ public:
         cusparseSetMatType(descr_, CUSPARSE_MATRIX_TYPE_GENERAL);
         cusparseSetMatIndexBase(descr_, CUSPARSE_INDEX_BASE_ZERO);
         d_err_.resize(2);
+        cuda_check(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (auto &e : ev_) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
     }
     ~MfSolver()
     {
+        drop_graphs();
+        for (auto &e : ev_)
+            if (e) cudaEventDestroy(e);
+        if (cap_) cudaStreamDestroy(cap_);
         if (descr_) cusparseDestroyMatDescr(descr_);
         if (hsp_) cusolverSpDestroy(hsp_);
     }
@@ -516,11 +528,16 @@ public:
     int64_t factor_nonzeros() const { return sym_.factor_nnz; }
     const MfSymbolic &symbolic() const { return sym_; }
     int big_fronts() const { return (int)big_list_.size(); }
+    double factor_ms() const { return factor_ms_; }
+    double solve_ms() const { return solve_ms_; }
+    int64_t solves() const { return n_solves_; }
+    void set_profile(bool p) { profile_ = p; }
     int n() const { return sym_.n; }
 
     void analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block)
     {
         analyzed_ = factored_ = false;
+        drop_graphs();
         std::string e = sym_.analyze(n, col_ptr, row_idx, block, hsp_, descr_);
         if (!e.empty()) throw Failure(IFEA_INPUT_INVALID, e);
         const MfSymbolic &S = sym_;
@@ -614,61 +631,33 @@ public:
         analyzed_ = true;
     }
 
-    // Numeric factorisation of device values in the order of the analysed full CSC pattern.
+    // Numeric factorisation of device values in the order of the analysed full CSC pattern. The launch sequence
+    // depends only on the pattern, so it is captured once (per values buffer) as a CUDA graph and replayed.
     void factorize(const double *d_full_vals)
     {
         if (!analyzed_) throw Failure(IFEA_BAD_STATE, "Analyze must be called first.");
         factored_ = false;
         const MfSymbolic &S = sym_;
-        int32_t init[2] = {INT_MAX, 0};
-        cuda_check(cudaMemcpyAsync(d_err_.p, init, sizeof init, cudaMemcpyHostToDevice, st_), "H2D");
-        for (int l = 0; l < S.nlevels; l++) {
-            int64_t p0 = S.level_pool_start[l], p1 = S.level_pool_start[l + 1];
-            cuda_check(cudaMemsetAsync(d_F_.p + p0, 0, (size_t)(p1 - p0) * sizeof(double), st_), "memset fronts");
-            int64_t a0 = S.a_level_start[l], a1 = S.a_level_start[l + 1];
-            if (a1 > a0) {
-                int g = (int)std::min<int64_t>((a1 - a0 + 255) / 256, 4 * 148);
-                mf::k_scatter<<<g, 256, 0, st_>>>(a1 - a0, d_adst_.p + a0, d_asrc_.p + a0, d_full_vals, d_F_);
-            }
-            for (int r = 0; r < S.max_rank; r++) {
-                int32_t e0 = S.ext_start[(size_t)l * S.max_rank + r], e1 = S.ext_start[(size_t)l * S.max_rank + r + 1];
-                if (e1 <= e0) continue;
-                dim3 grid(64, e1 - e0);
-                mf::k_extend<<<grid, 128, 0, st_>>>(dev_, d_ext_.p + e0, d_par_);
-            }
-            int q0 = S.level_start[l], q1 = S.level_start[l + 1];
-            int maxc = S.ncol[lvl_sorted_[q0]];
-            for (int k0 = 0; k0 < maxc; k0 += mf::PW) {
-                int cnt = 0, maxt = 0, maxr = 0;
-                for (int q = q0; q < q1 && S.ncol[lvl_sorted_[q]] > k0; q++) {
-                    int s = lvl_sorted_[q];
-                    cnt++;
-                    int w = std::min(mf::PW, S.ncol[s] - k0), nt = S.m[s] - k0 - w;
-                    int nti = (nt + mf::UT - 1) / mf::UT;
-                    maxt = std::max(maxt, nti * (nti + 1) / 2);
-                    maxr = std::max(maxr, (nt + mf::PW - 1) / mf::PW);
-                }
-                mf::k_panel<<<cnt, 256, 0, st_>>>(dev_, d_lvl_.p + q0, k0, d_err_);
-                if (maxr > 0) mf::k_panel_trsm<<<dim3(maxr, cnt), 256, kPairSmem, st_>>>(dev_, d_lvl_.p + q0, k0);
-                if (maxt > 0) {
-                    dim3 grid(std::min(maxt, 4096), cnt);
-                    mf::k_update<<<grid, 256, kUpdateSmem, st_>>>(dev_, d_lvl_.p + q0, k0);
-                }
-            }
-            int b0 = big_start_[l], b1 = big_start_[l + 1];
-            if (b1 > b0) {
-                int nbmax = (S.ncol[big_list_[b0]] + mf::PW - 1) / mf::PW;
-                for (int bi = 0; bi < nbmax; bi++) {
-                    int cnt = 0;
-                    while (b0 + cnt < b1 && (S.ncol[big_list_[b0 + cnt]] + mf::PW - 1) / mf::PW > bi) cnt++;
-                    mf::k_inverse_row<<<dim3(bi + 1, cnt), 256, kPairSmem, st_>>>(dev_, d_big_.p + b0, bi);
-                }
-            }
+        if (!factor_exec_ || factor_vals_ != d_full_vals) {
+            if (factor_exec_) cudaGraphExecDestroy(factor_exec_);
+            factor_exec_ = nullptr;
+            cudaGraph_t g = nullptr;
+            cuda_check(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+            enqueue_factor(cap_, d_full_vals);
+            cuda_check(cudaStreamEndCapture(cap_, &g), "cudaStreamEndCapture");
+            cudaError_t e = cudaGraphInstantiate(&factor_exec_, g, 0);
+            cudaGraphDestroy(g);
+            cuda_check(e, "cudaGraphInstantiate");
+            factor_vals_ = d_full_vals;
         }
-        cuda_check(cudaGetLastError(), "multifrontal factorisation launch");
+        cuda_check(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
+        cuda_check(cudaGraphLaunch(factor_exec_, st_), "cudaGraphLaunch");
+        cuda_check(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
         int32_t e[2];
         cuda_check(cudaMemcpyAsync(e, d_err_.p, sizeof e, cudaMemcpyDeviceToHost, st_), "D2H");
         cuda_check(cudaStreamSynchronize(st_), "cudaStreamSynchronize");
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, ev_[0], ev_[1]) == cudaSuccess) factor_ms_ += ms;
         if (e[0] != INT_MAX) {
             int row = S.perm[e[0]];
             throw Failure(IFEA_NOT_SPD, "Stiffness matrix not positive definite at equation " + std::to_string(row) +
@@ -677,16 +666,92 @@ public:
         factored_ = true;
     }
 
-    // x = A^-1 b on the device (b and x may alias).
+    void enqueue_factor(cudaStream_t st, const double *d_full_vals)
+    {
+        const MfSymbolic &S = sym_;
+        mf::k_init_err<<<1, 1, 0, st>>>(d_err_);
+        for (int l = 0; l < S.nlevels; l++) {
+            int64_t p0 = S.level_pool_start[l], p1 = S.level_pool_start[l + 1];
+            cuda_check(cudaMemsetAsync(d_F_.p + p0, 0, (size_t)(p1 - p0) * sizeof(double), st), "memset fronts");
+            int64_t a0 = S.a_level_start[l], a1 = S.a_level_start[l + 1];
+            if (a1 > a0) {
+                int g = (int)std::min<int64_t>((a1 - a0 + 255) / 256, 4 * 148);
+                mf::k_scatter<<<g, 256, 0, st>>>(a1 - a0, d_adst_.p + a0, d_asrc_.p + a0, d_full_vals, d_F_);
+            }
+            for (int r = 0; r < S.max_rank; r++) {
+                int32_t e0 = S.ext_start[(size_t)l * S.max_rank + r], e1 = S.ext_start[(size_t)l * S.max_rank + r + 1];
+                if (e1 <= e0) continue;
+                dim3 grid(64, e1 - e0);
+                mf::k_extend<<<grid, 128, 0, st>>>(dev_, d_ext_.p + e0, d_par_);
+            }
+            int q0 = S.level_start[l], q1 = S.level_start[l + 1];
+            int maxc = S.ncol[lvl_sorted_[q0]];
+            for (int k0 = 0; k0 < maxc; k0 += mf::PW) {
+                int cnt = 0, maxt = 0, maxr = 0;
+                for (int q = q0; q < q1 && S.ncol[lvl_sorted_[q]] > k0; q++) {
+                    int sn = lvl_sorted_[q];
+                    cnt++;
+                    int w = std::min(mf::PW, S.ncol[sn] - k0), nt = S.m[sn] - k0 - w;
+                    int nti = (nt + mf::UT - 1) / mf::UT;
+                    maxt = std::max(maxt, nti * (nti + 1) / 2);
+                    maxr = std::max(maxr, (nt + mf::PW - 1) / mf::PW);
+                }
+                mf::k_panel<<<cnt, 256, 0, st>>>(dev_, d_lvl_.p + q0, k0, d_err_);
+                if (maxr > 0) mf::k_panel_trsm<<<dim3(maxr, cnt), 256, kPairSmem, st>>>(dev_, d_lvl_.p + q0, k0);
+                if (maxt > 0) {
+                    dim3 grid(std::min(maxt, 4096), cnt);
+                    mf::k_update<<<grid, 256, kUpdateSmem, st>>>(dev_, d_lvl_.p + q0, k0);
+                }
+            }
+            int b0 = big_start_[l], b1 = big_start_[l + 1];
+            if (b1 > b0) {
+                int nbmax = (S.ncol[big_list_[b0]] + mf::PW - 1) / mf::PW;
+                for (int bi = 0; bi < nbmax; bi++) {
+                    int cnt = 0;
+                    while (b0 + cnt < b1 && (S.ncol[big_list_[b0 + cnt]] + mf::PW - 1) / mf::PW > bi) cnt++;
+                    mf::k_inverse_row<<<dim3(bi + 1, cnt), 256, kPairSmem, st>>>(dev_, d_big_.p + b0, bi);
+                }
+            }
+        }
+        cuda_check(cudaGetLastError(), "multifrontal factorisation launch");
+    }
+
+    // x = A^-1 b on the device (b and x may alias). The level sweeps run as one captured CUDA graph on the
+    // solver's internal vector; only the permutations in and out are launched per call.
     void solve(const double *d_b, double *d_x)
     {
         if (!factored_) throw Failure(IFEA_BAD_STATE, "Factorize must be called first.");
         const MfSymbolic &S = sym_;
         int n = S.n, g = std::max(1, std::min((n + 255) / 256, 4 * 148));
+        if (!solve_exec_) {
+            cudaGraph_t gr = nullptr;
+            cuda_check(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+            enqueue_sweeps(cap_);
+            cuda_check(cudaStreamEndCapture(cap_, &gr), "cudaStreamEndCapture");
+            cudaError_t e = cudaGraphInstantiate(&solve_exec_, gr, 0);
+            cudaGraphDestroy(gr);
+            cuda_check(e, "cudaGraphInstantiate");
+        }
+        if (profile_) cuda_check(cudaEventRecord(ev_[2], st_), "cudaEventRecord");
         mf::k_permute_in<<<g, 256, 0, st_>>>(n, d_perm_, d_b, d_y_);
+        cuda_check(cudaGraphLaunch(solve_exec_, st_), "cudaGraphLaunch");
+        mf::k_permute_out<<<g, 256, 0, st_>>>(n, d_perm_, d_y_, d_x);
+        n_solves_++;
+        if (profile_) {
+            cuda_check(cudaEventRecord(ev_[3], st_), "cudaEventRecord");
+            cuda_check(cudaEventSynchronize(ev_[3]), "cudaEventSynchronize");
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, ev_[2], ev_[3]) == cudaSuccess) solve_ms_ += ms;
+        }
+        cuda_check(cudaGetLastError(), "multifrontal solve launch");
+    }
+
+    void enqueue_sweeps(cudaStream_t st)
+    {
+        const MfSymbolic &S = sym_;
         for (int l = 0; l < S.nlevels; l++) {
             int q0 = small_start_[l], cnt = small_start_[l + 1] - q0;
-            if (cnt > 0) mf::k_forward<<<cnt, 512, small_smem_, st_>>>(dev_, d_small_.p + q0, d_y_);
+            if (cnt > 0) mf::k_forward<<<cnt, 512, small_smem_, st>>>(dev_, d_small_.p + q0, d_y_);
             int b0 = big_start_[l], bc = big_start_[l + 1] - b0;
             if (bc > 0) {
                 int mnc = 1, mnr = 1;
@@ -694,24 +759,21 @@ public:
                     mnc = std::max(mnc, S.ncol[big_list_[q]]);
                     mnr = std::max(mnr, S.m[big_list_[q]] - S.ncol[big_list_[q]]);
                 }
-                mf::k_wide_fwd_acc<<<bc, 512, 0, st_>>>(dev_, d_big_.p + b0, d_y_);
-                mf::k_wide_fwd_y<<<dim3((mnc + 31) / 32, bc), 256, 0, st_>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
-                mf::k_wide_fwd_t<<<dim3((mnr + 31) / 32, bc), 256, 0, st_>>>(dev_, d_big_.p + b0, d_y1_);
+                mf::k_wide_fwd_acc<<<bc, 512, 0, st>>>(dev_, d_big_.p + b0, d_y_);
+                mf::k_wide_fwd_y<<<dim3((mnc + 31) / 32, bc), 256, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
+                mf::k_wide_fwd_t<<<dim3((mnr + 31) / 32, bc), 256, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
             }
         }
-        // back substitution writes x (new numbering) in place of y, top level first
         for (int l = S.nlevels - 1; l >= 0; l--) {
             int q0 = small_start_[l], cnt = small_start_[l + 1] - q0;
-            if (cnt > 0) mf::k_backward<<<cnt, 512, small_smem_, st_>>>(dev_, d_small_.p + q0, d_y_, d_y_);
+            if (cnt > 0) mf::k_backward<<<cnt, 512, small_smem_, st>>>(dev_, d_small_.p + q0, d_y_, d_y_);
             int b0 = big_start_[l], bc = big_start_[l + 1] - b0;
             if (bc > 0) {
                 int mnc = S.ncol[big_list_[b0]];
-                mf::k_wide_bwd_z<<<dim3((mnc + 7) / 8, bc), 256, 0, st_>>>(dev_, d_big_.p + b0, d_y_, d_z_);
-                mf::k_wide_bwd_x<<<dim3((mnc + 7) / 8, bc), 256, 0, st_>>>(dev_, d_big_.p + b0, d_z_, d_y_);
+                mf::k_wide_bwd_z<<<dim3((mnc + 7) / 8, bc), 256, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_z_);
+                mf::k_wide_bwd_x<<<dim3((mnc + 7) / 8, bc), 256, 0, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
             }
         }
-        mf::k_permute_out<<<g, 256, 0, st_>>>(n, d_perm_, d_y_, d_x);
-        cuda_check(cudaGetLastError(), "multifrontal solve launch");
     }
 
     void check_finite(const double *d_x)
@@ -725,6 +787,20 @@ public:
     }
 
 private:
+    void drop_graphs()
+    {
+        if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
+        if (factor_exec_) cudaGraphExecDestroy(factor_exec_);
+        solve_exec_ = factor_exec_ = nullptr;
+        factor_vals_ = nullptr;
+    }
+    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+    double factor_ms_ = 0, solve_ms_ = 0;
+    int64_t n_solves_ = 0;
+    bool profile_ = false;
+    cudaStream_t cap_ = nullptr;
+    cudaGraphExec_t solve_exec_ = nullptr, factor_exec_ = nullptr;
+    const double *factor_vals_ = nullptr;
     static constexpr size_t kUpdateSmem = 2 * mf::UT * (mf::PW + 1) * sizeof(double);
     static constexpr size_t kPairSmem = 2 * mf::PW * (mf::PW + 1) * sizeof(double);
     cudaStream_t st_;

@@ -689,6 +689,7 @@ struct Forging3D {
         S("t_factor", t_factor) S("t_pcg", t_pcg) S("t_final", t_final) S("t_update", t_update) S("t_total", t_total)
         S("supernodes", lin->symbolic().nsuper) S("levels", lin->symbolic().nlevels)
         S("front_pool_mb", lin->symbolic().pool * 8e-6) S("max_front", lin->symbolic().max_m) S("big_fronts", lin->big_fronts())
+        S("factor_gpu_ms", lin->factor_ms()) S("solve_gpu_ms", lin->solve_ms()) S("solves", lin->solves())
 #undef S
         if (nm == "volume") return volume();
         if (nm == "min_quality") return min_quality(d_x);
@@ -700,6 +701,7 @@ struct Forging3D {
         else if (nm == "recovery_pass") recovery_pass = (int)v;
         else if (nm == "ds_cur") ds_cur = v;
         else if (nm == "warm") warm = (int)v;
+        else if (nm == "profile_solves") lin->set_profile(v != 0);
         else throw Failure(IFEA_INPUT_INVALID, "unknown scalar name '" + nm + "'");
     }
 };
