@@ -59,69 +59,89 @@ static __global__ void k_extend(Dev D, const int32_t *__restrict__ children, con
     }
 }
 
-// Panel k0 of every listed front: Cholesky of the diagonal block in shared memory, the block's inverse (kept for
-// the solves), then the rows below: X = F21 L11^-T, as a triangular matrix-vector product per row. The lowest
-// failing pivot column (new numbering) goes to err.
+// Panel k0 of every listed front: Cholesky of the diagonal block in shared memory and the block's inverse (kept
+// for the rows below and for the solves). The factorisation runs in the L D L^T form (the pivot column is scaled
+// only at the end), so each column costs one barrier; rows at or beyond the block width are padded with the
+// identity. The inverse is built by recursive doubling: the 8x8 diagonal blocks are inverted by forward
+// substitution in registers, then pairs of blocks merge with X21 = -X22 L21 X11 at sizes 8, 16 and 32. The lowest
+// failing pivot column (new numbering) goes to err. Dynamic shared memory: two 64 x 65 blocks and a 32 x 33 one.
 static __global__ void __launch_bounds__(256) k_panel(Dev D, const int32_t *__restrict__ fronts, int k0, int *err)
 {
-    __shared__ double Ds[PW][PW + 1];
-    __shared__ int bad;
+    extern __shared__ double shp[];
+    double (*Ds)[PW + 1] = (double (*)[PW + 1])shp;
+    double (*Xs)[PW + 1] = (double (*)[PW + 1])(shp + PW * (PW + 1));
+    double (*Ts)[33] = (double (*)[33])(shp + 2 * PW * (PW + 1));
+    __shared__ double sq[PW];
     int s = fronts[blockIdx.x];
     int ms = D.m[s], w = min(PW, D.ncol[s] - k0);
     double *F = D.F + D.front_off[s];
     double *Inv = D.Inv + D.inv_off[s] + (int64_t)(k0 / PW) * PW * PW;
-    int tid = threadIdx.x, nt = blockDim.x;
-    if (tid == 0) bad = 0;
-    for (int t = tid; t < w * w; t += nt) {
-        int r = t / w, c = t % w;
-        if (r >= c) Ds[r][c] = F[(int64_t)(k0 + c) * ms + k0 + r];
+    int tid = threadIdx.x, r = tid & (PW - 1), cg = tid >> 6;
+    for (int t = tid; t < PW * PW; t += blockDim.x) {
+        int rr = t % PW, c = t / PW;
+        double v = rr == c ? 1.0 : 0.0;
+        if (rr < w && c < w && rr >= c) v = F[(int64_t)(k0 + c) * ms + k0 + rr];
+        Ds[rr][c] = v;
+        Xs[rr][c] = 0.0;
     }
     __syncthreads();
     for (int k = 0; k < w; k++) {
-        if (tid == 0) {
-            double d = Ds[k][k];
-            if (!(d > 0)) {
-                bad = 1;
-                atomicMin(err, D.c0[s] + k0 + k);
-            } else {
-                Ds[k][k] = sqrt(d);
-            }
+        double d = Ds[k][k];
+        if (!(d > 0)) {
+            if (tid == 0) atomicMin(err, D.c0[s] + k0 + k);
+            return;  // every thread read the same pivot: a uniform exit
         }
-        __syncthreads();
-        if (bad) return;
-        double lkk = Ds[k][k];
-        for (int r = k + 1 + tid; r < w; r += nt) Ds[r][k] /= lkk;
-        __syncthreads();
-        int mm = w - k - 1;
-        for (int t = tid; t < mm * (mm + 1) / 2; t += nt) {
-            int di = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-            while ((di + 1) * (di + 2) / 2 <= t) di++;
-            while (di * (di + 1) / 2 > t) di--;
-            int dj = t - di * (di + 1) / 2;
-            int r = k + 1 + di, c = k + 1 + dj;
-            Ds[r][c] -= Ds[r][k] * Ds[c][k];
+        if (r > k) {
+            double a = Ds[r][k] / d;
+            for (int c = k + 1 + cg; c <= r; c += 4) Ds[r][c] -= a * Ds[c][k];
         }
         __syncthreads();
     }
-    for (int t = tid; t < w * w; t += nt) {
-        int r = t / w, c = t % w;
-        if (r >= c) F[(int64_t)(k0 + c) * ms + k0 + r] = Ds[r][c];
-    }
-    // inverse of the lower-triangular block, column t by thread t (forward substitution on e_t)
-    if (tid < w) {
-        double x[PW];
-        for (int i = 0; i < tid; i++) x[i] = 0.0;
-        x[tid] = 1.0 / Ds[tid][tid];
-        for (int i = tid + 1; i < w; i++) {
-            double v = 0;
-            for (int k = tid; k < i; k++) v += Ds[i][k] * x[k];
-            x[i] = -v / Ds[i][i];
-        }
-        for (int i = 0; i < PW; i++) Inv[(int64_t)tid * PW + i] = i < w ? x[i] : 0.0;  // column-major, row i
-    }
-    for (int t = tid; t < PW * PW; t += nt)
-        if (t / PW >= w) Inv[t] = 0.0;
+    if (tid < PW) sq[tid] = sqrt(Ds[tid][tid]);
     __syncthreads();
+    for (int c = cg; c <= r; c += 4) Ds[r][c] = c == r ? sq[r] : Ds[r][c] / sq[c];
+    __syncthreads();
+    for (int t = tid; t < w * w; t += blockDim.x) {
+        int rr = t % w, c = t / w;
+        if (rr >= c) F[(int64_t)(k0 + c) * ms + k0 + rr] = Ds[rr][c];
+    }
+    // 8x8 diagonal blocks: thread (b, j) forward-substitutes column j of block b
+    if (tid < PW) {
+        int b8 = (tid >> 3) * 8, j = tid & 7;
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            double v = i == j ? 1.0 : 0.0;
+#pragma unroll
+            for (int q = 0; q < i; q++) v -= Ds[b8 + i][b8 + q] * x[q];
+            x[i] = v / Ds[b8 + i][b8 + i];
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) Xs[b8 + i][b8 + j] = x[i];
+    }
+    __syncthreads();
+    for (int h = 8; h < PW; h *= 2) {
+        // T = L21 X11 for every pair (rows b+h.., columns b..), X11 lower triangular
+        int per = h * h, total = (PW / (2 * h)) * per;
+        for (int t = tid; t < total; t += blockDim.x) {
+            int p = t / per, e = t % per, i = e / h, j = e % h, b = p * 2 * h;
+            double v = 0;
+            for (int q = j; q < h; q++) v += Ds[b + h + i][b + q] * Xs[b + q][b + j];
+            Ts[p * h + i][j] = v;  // the pairs of one size fill 32 rows
+        }
+        __syncthreads();
+        for (int t = tid; t < total; t += blockDim.x) {
+            int p = t / per, e = t % per, i = e / h, j = e % h, b = p * 2 * h;
+            double v = 0;
+            for (int q = 0; q <= i; q++) v += Xs[b + h + i][b + h + q] * Ts[p * h + q][j];
+            Xs[b + h + i][b + j] = -v;
+        }
+        __syncthreads();
+    }
+    for (int t = tid; t < PW * PW; t += blockDim.x) {
+        int i = t % PW, c = t / PW;
+        Inv[t] = (i < w && c < w) ? Xs[i][c] : 0.0;  // column-major, row i
+    }
 }
 
 // Rows below the diagonal block of panel k0, 64 rows per CTA: X = F21 L11^-T = F21 Dinv^T, i.e.
@@ -165,39 +185,55 @@ static __global__ void __launch_bounds__(256) k_panel_trsm(Dev D, const int32_t 
         }
 }
 
-// Block row bi of the full inverse X = L11^-1 of every listed wide supernode (column-major ncol x ncol), one CTA
-// per (block column j <= bi, front): X_ii = Dinv_i, X_ij = -Dinv_i sum_{k=j}^{i-1} L_ik X_kj.
-static __global__ void __launch_bounds__(256) k_inverse_row(Dev D, const int32_t *__restrict__ fronts, int bi)
+// Full inverse X = L11^-1 of the pivot block of the wide supernodes (column-major ncol x ncol), by recursive
+// doubling over 64-column blocks. The diagonal blocks are the panel inverses (k_xinv_diag). Then groups of 2^t
+// blocks merge their halves, top [g0, gm) and bottom [gm, g1): X21 = -X22 L21 X11, in two passes over the
+// 64 x 64 output tiles (bi in the bottom half, bj in the top half): T = L21 X11 (k_xinv_gemm<0>, stored transposed
+// in X's unused upper triangle), then X21 = -X22 T (k_xinv_gemm<1>). The tasks (front, bi, bj, gm) of one pass are
+// listed on the host; one CTA per task, each thread a 4 x 4 register block.
+static __global__ void k_xinv_diag(Dev D, const int4 *__restrict__ tasks)
+{
+    int4 tk = tasks[blockIdx.x];
+    int s = tk.x, bi = tk.y, nc = D.ncol[s], r0 = bi * PW, w = min(PW, nc - r0);
+    const double *Dinv = D.Inv + D.inv_off[s] + (int64_t)bi * PW * PW;
+    double *X = D.Xinv + D.xinv_off[s];
+    for (int t = threadIdx.x; t < PW * PW; t += blockDim.x) {
+        int c = t / PW, r = t % PW;
+        if (r < w && c < w) X[(int64_t)(r0 + c) * nc + r0 + r] = Dinv[t];
+    }
+}
+
+template <int PASS>
+static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev D, const int4 *__restrict__ tasks)
 {
     extern __shared__ double shm[];
     double (*A)[PW + 1] = (double (*)[PW + 1])shm;
     double (*B)[PW + 1] = (double (*)[PW + 1])(shm + PW * (PW + 1));
-    int s = fronts[blockIdx.y];
-    int bj = blockIdx.x;
-    if (bj > bi) return;
+    int4 tk = tasks[blockIdx.x];
+    int s = tk.x, bi = tk.y, bj = tk.z, gm = tk.w;
     int ms = D.m[s], nc = D.ncol[s];
     const double *F = D.F + D.front_off[s];
     double *X = D.Xinv + D.xinv_off[s];
     int r0 = bi * PW, c0 = bj * PW, wr = min(PW, nc - r0), wc = min(PW, nc - c0);
-    const double *Dinv_i = D.Inv + D.inv_off[s] + (int64_t)bi * PW * PW;
+    int kb0 = PASS == 0 ? bj : gm, kb1 = PASS == 0 ? gm : bi + 1;
     int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    if (bj == bi) {
-        for (int t = threadIdx.x; t < PW * PW; t += blockDim.x) {
-            int c = t / PW, r = t % PW;
-            if (r < wr && c < wc) X[(int64_t)(c0 + c) * nc + r0 + r] = Dinv_i[t];
-        }
-        return;
-    }
     double acc[4][4];
     for (int a = 0; a < 4; a++)
         for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
-    for (int bk = bj; bk < bi; bk++) {
+    for (int bk = kb0; bk < kb1; bk++) {
         int k0 = bk * PW, wk = min(PW, nc - k0);
         __syncthreads();
         for (int t = threadIdx.x; t < PW * PW; t += blockDim.x) {
-            int k = t / PW, r = t % PW;
-            A[r][k] = (r < wr && k < wk) ? F[(int64_t)(k0 + k) * ms + r0 + r] : 0.0;
-            B[r][k] = (r < wk && k < wc) ? X[(int64_t)(c0 + k) * nc + k0 + r] : 0.0;
+            int lo = t % PW, hi = t / PW;  // lo runs along contiguous memory
+            // A(r = lo, k = hi): pass 0 L(bi, bk) from the front, pass 1 X(bi, bk)
+            bool oka = lo < wr && hi < wk;
+            A[lo][hi] = !oka       ? 0.0
+                        : PASS == 0 ? F[(int64_t)(k0 + hi) * ms + r0 + lo]
+                                    : X[(int64_t)(k0 + hi) * nc + r0 + lo];
+            if (PASS == 0)  // B(k = lo, c = hi) = X(bk, bj)
+                B[lo][hi] = (lo < wk && hi < wc) ? X[(int64_t)(c0 + hi) * nc + k0 + lo] : 0.0;
+            else  // B(k = hi, c = lo) = T(bk, bj), stored at X(c0 + c, k0 + k)
+                B[hi][lo] = (hi < wk && lo < wc) ? X[(int64_t)(k0 + hi) * nc + c0 + lo] : 0.0;
         }
         __syncthreads();
         for (int k = 0; k < PW; k++) {
@@ -208,27 +244,14 @@ static __global__ void __launch_bounds__(256) k_inverse_row(Dev D, const int32_t
                 for (int b = 0; b < 4; b++) acc[a][b] += a4[a] * b4[b];
         }
     }
-    __syncthreads();
-    for (int a = 0; a < 4; a++)
-        for (int b = 0; b < 4; b++) B[tx + 16 * a][ty + 16 * b] = acc[a][b];
-    for (int t = threadIdx.x; t < PW * PW; t += blockDim.x) {
-        int c = t / PW, r = t % PW;
-        A[r][c] = Dinv_i[t];
-    }
-    __syncthreads();
-    for (int a = 0; a < 4; a++)
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
-    for (int k = 0; k < PW; k++) {
-        double a4[4], b4[4];
-        for (int a = 0; a < 4; a++) a4[a] = A[tx + 16 * a][k];
-        for (int b = 0; b < 4; b++) b4[b] = B[k][ty + 16 * b];
-        for (int a = 0; a < 4; a++)
-            for (int b = 0; b < 4; b++) acc[a][b] += a4[a] * b4[b];
-    }
     for (int a = 0; a < 4; a++)
         for (int b = 0; b < 4; b++) {
             int r = tx + 16 * a, c = ty + 16 * b;
-            if (r < wr && c < wc) X[(int64_t)(c0 + c) * nc + r0 + r] = -acc[a][b];
+            if (r >= wr || c >= wc) continue;
+            if (PASS == 0)
+                X[(int64_t)(r0 + r) * nc + c0 + c] = acc[a][b];  // T(r, c) stored at X(c0 + c, r0 + r)
+            else
+                X[(int64_t)(c0 + c) * nc + r0 + r] = -acc[a][b];
         }
 }
 
@@ -253,83 +276,108 @@ static __global__ void k_wide_fwd_acc(Dev D, const int32_t *__restrict__ fronts,
     }
 }
 
-// y1 = X acc1: 32 rows per CTA (blockIdx.x), 8 warps splitting the columns; front = blockIdx.y.
-static __global__ void __launch_bounds__(256) k_wide_fwd_y(Dev D, const int32_t *__restrict__ fronts, double *y, double *Y1)
+// The row-oriented GEMVs below give each CTA 16 rows and let its 16 warps split the columns: a half-warp reads
+// 16 consecutive rows of one column (128 contiguous bytes), the 32 half-warps of the CTA take columns
+// sub, sub + 32, ... so every thread keeps several independent loads in flight. Row tiles are visited bottom-up
+// (the longest rows of a triangular operand first).
+constexpr int RT = 16;
+
+// y1 = X acc1 (X lower triangular).
+static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev D, const int32_t *__restrict__ fronts, double *y, double *Y1)
 {
-    __shared__ double part[8][33];
+    __shared__ double part[32][RT + 1];
     int s = fronts[blockIdx.y];
-    int nc = D.ncol[s], c0 = D.c0[s];
-    if (blockIdx.x * 32 >= nc) return;
+    int nc = D.ncol[s], c0 = D.c0[s], ntile = (nc + RT - 1) / RT;
+    if ((int)blockIdx.x >= ntile) return;
+    int r0 = (ntile - 1 - blockIdx.x) * RT;
     const double *X = D.Xinv + D.xinv_off[s];
     const double *acc = D.Abig + D.idx_start[s];
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int r = blockIdx.x * 32 + lane;
+    int lane = threadIdx.x & 31, sub = (lane >> 4) + 2 * (threadIdx.x >> 5), rr = lane & (RT - 1);
+    int r = r0 + rr, cend = min(nc, r0 + RT);
     double v = 0;
-    if (r < nc)
-        for (int c = warp; c <= r; c += 8) v += X[(int64_t)c * nc + r] * acc[c];
-    part[warp][lane] = v;
+    if (r < nc) {
+#pragma unroll 8
+        for (int c = sub; c < cend; c += 32)
+            if (c <= r) v += X[(int64_t)c * nc + r] * acc[c];
+    }
+    part[sub][rr] = v;
     __syncthreads();
-    if (warp == 0 && r < nc) {
+    if (threadIdx.x < RT && r0 + (int)threadIdx.x < nc) {
         double t = 0;
-        for (int w = 0; w < 8; w++) t += part[w][lane];
-        y[c0 + r] = t;
-        Y1[D.idx_start[s] + r] = t;
+        for (int q = 0; q < 32; q++) t += part[q][threadIdx.x];
+        y[c0 + r0 + threadIdx.x] = t;
+        Y1[D.idx_start[s] + r0 + threadIdx.x] = t;
     }
 }
 
-// update vector t = -acc2 + L21 y1: 32 rows per CTA, 8 warps splitting the pivot columns.
-static __global__ void __launch_bounds__(256) k_wide_fwd_t(Dev D, const int32_t *__restrict__ fronts, const double *Y1)
+// update vector t = -acc2 + L21 y1.
+static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev D, const int32_t *__restrict__ fronts, const double *Y1)
 {
-    __shared__ double part[8][33];
+    __shared__ double part[32][RT + 1];
     int s = fronts[blockIdx.y];
     int ms = D.m[s], nc = D.ncol[s], nr = ms - nc;
-    if (blockIdx.x * 32 >= nr) return;
-    const double *F = D.F + D.front_off[s];
+    int i0 = blockIdx.x * RT;
+    if (i0 >= nr) return;
+    const double *F = D.F + D.front_off[s] + nc;
     const double *y1 = Y1 + D.idx_start[s];
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int i = blockIdx.x * 32 + lane;
+    int lane = threadIdx.x & 31, sub = (lane >> 4) + 2 * (threadIdx.x >> 5), rr = lane & (RT - 1);
+    int i = i0 + rr;
     double v = 0;
-    if (i < nr)
-        for (int k = warp; k < nc; k += 8) v += F[(int64_t)k * ms + nc + i] * y1[k];
-    part[warp][lane] = v;
+    if (i < nr) {
+#pragma unroll 8
+        for (int k = sub; k < nc; k += 32) v += F[(int64_t)k * ms + i] * y1[k];
+    }
+    part[sub][rr] = v;
     __syncthreads();
-    if (warp == 0 && i < nr) {
+    if (threadIdx.x < RT && i0 + (int)threadIdx.x < nr) {
         double t = 0;
-        for (int w = 0; w < 8; w++) t += part[w][lane];
-        D.U[D.uvec_start[s] + i] = -D.Abig[D.idx_start[s] + nc + i] + t;
+        for (int q = 0; q < 32; q++) t += part[q][threadIdx.x];
+        int ii = i0 + threadIdx.x;
+        D.U[D.uvec_start[s] + ii] = -D.Abig[D.idx_start[s] + nc + ii] + t;
     }
 }
 
-// z = y1 - L21^T x2, one warp per pivot column.
-static __global__ void __launch_bounds__(256) k_wide_bwd_z(Dev D, const int32_t *__restrict__ fronts, const double *x, double *Z)
+// z = y1 - L21^T x2, one warp per pivot column; x2 is gathered into shared memory once per CTA.
+static __global__ void __launch_bounds__(512) k_wide_bwd_z(Dev D, const int32_t *__restrict__ fronts, const double *x, double *Z)
 {
+    extern __shared__ double xs[];
     int s = fronts[blockIdx.y];
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s], nr = ms - nc;
-    int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int kbase = blockIdx.x * (blockDim.x >> 5);
+    if (kbase >= nc) return;
+    const int32_t *ix = D.idx + D.idx_start[s] + nc;
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) xs[i] = x[ix[i]];
+    __syncthreads();
+    int k = kbase + (threadIdx.x >> 5);
     if (k >= nc) return;
-    const double *F = D.F + D.front_off[s];
-    const int32_t *ix = D.idx + D.idx_start[s];
+    const double *col = D.F + D.front_off[s] + (int64_t)k * ms + nc;
     int lane = threadIdx.x & 31;
-    const double *col = F + (int64_t)k * ms + nc;
     double v = 0;
-    for (int i = lane; i < nr; i += 32) v += col[i] * x[ix[nc + i]];
+#pragma unroll 8
+    for (int i = lane; i < nr; i += 32) v += col[i] * xs[i];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) Z[D.idx_start[s] + k] = x[c0 + k] - v;
 }
 
-// x1 = X^T z, one warp per pivot column j (column j of X is contiguous).
-static __global__ void __launch_bounds__(256) k_wide_bwd_x(Dev D, const int32_t *__restrict__ fronts, const double *Z, double *x)
+// x1 = X^T z, one warp per pivot column j (column j of X is contiguous); z is staged in shared memory.
+static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev D, const int32_t *__restrict__ fronts, const double *Z, double *x)
 {
+    extern __shared__ double zs[];
     int s = fronts[blockIdx.y];
     int nc = D.ncol[s], c0 = D.c0[s];
-    int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (j >= nc) return;
-    const double *X = D.Xinv + D.xinv_off[s];
+    int nw = blockDim.x >> 5, nblk = (nc + nw - 1) / nw;
+    if ((int)blockIdx.x >= nblk) return;
+    int jbase = (nblk - 1 - blockIdx.x) * nw;  // leftmost (longest) columns first
     const double *z = Z + D.idx_start[s];
+    for (int i = jbase + threadIdx.x; i < nc; i += blockDim.x) zs[i - jbase] = z[i];
+    __syncthreads();
+    int j = jbase + (threadIdx.x >> 5);
+    if (j >= nc) return;
+    const double *col = D.Xinv + D.xinv_off[s] + (int64_t)j * nc;
     int lane = threadIdx.x & 31;
-    const double *col = X + (int64_t)j * nc;
     double v = 0;
-    for (int i = j + lane; i < nc; i += 32) v += col[i] * z[i];
+#pragma unroll 8
+    for (int i = j + lane; i < nc; i += 32) v += col[i] * zs[i - jbase];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) x[c0 + j] = v;
 }
@@ -603,6 +651,46 @@ public:
             std::stable_sort(big_list_.begin() + big_start_[l], big_list_.begin() + big_start_[l + 1],
                              [&](int a, int b) { return S.ncol[a] > S.ncol[b]; });
         d_big_.upload(big_list_, st_);
+        wide_smem_ = 8;
+        for (int sn : big_list_) wide_smem_ = std::max(wide_smem_, (size_t)std::max(S.ncol[sn], S.m[sn] - S.ncol[sn]) * sizeof(double));
+        if (wide_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the wide solve kernels' shared-memory window");
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_wide_bwd_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wide_smem_), "cudaFuncSetAttribute");
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_wide_bwd_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wide_smem_), "cudaFuncSetAttribute");
+        // inverse passes of the wide supernodes, per level: diagonal copies, then for groups of 2, 4, ... blocks
+        // the T pass and the X21 pass
+        std::vector<int4> tasks;
+        xinv_pass_start_.assign(S.nlevels + 1, 0);
+        xinv_task_start_.assign(1, 0);
+        xinv_pass_kind_.clear();
+        auto close_pass = [&](int kind) {
+            if ((int)tasks.size() == xinv_task_start_.back()) return;
+            xinv_pass_kind_.push_back(kind);
+            xinv_task_start_.push_back((int)tasks.size());
+        };
+        for (int l = 0; l < S.nlevels; l++) {
+            xinv_pass_start_[l] = (int)xinv_pass_kind_.size();
+            int nbmax = 0;
+            for (int q = big_start_[l]; q < big_start_[l + 1]; q++) {
+                int sn = big_list_[q], nb = (S.ncol[sn] + mf::PW - 1) / mf::PW;
+                nbmax = std::max(nbmax, nb);
+                for (int b = 0; b < nb; b++) tasks.push_back(make_int4(sn, b, b, 0));
+            }
+            close_pass(0);
+            for (int G = 2; G / 2 < nbmax; G *= 2)
+                for (int kind = 1; kind <= 2; kind++) {
+                    for (int q = big_start_[l]; q < big_start_[l + 1]; q++) {
+                        int sn = big_list_[q], nb = (S.ncol[sn] + mf::PW - 1) / mf::PW;
+                        for (int g0 = 0; g0 + G / 2 < nb; g0 += G) {
+                            int gm = g0 + G / 2, g1 = std::min(g0 + G, nb);
+                            for (int bi = gm; bi < g1; bi++)
+                                for (int bj = g0; bj < gm; bj++) tasks.push_back(make_int4(sn, bi, bj, gm));
+                        }
+                    }
+                    close_pass(kind);
+                }
+        }
+        xinv_pass_start_[S.nlevels] = (int)xinv_pass_kind_.size();
+        d_xinv_tasks_.upload(tasks, st_);
         d_small_.upload(small_list_, st_);
         d_xinv_off_.upload(xinv_off_, st_);
         d_Xinv_.resize(std::max<int64_t>(xinv_total, 1));
@@ -620,9 +708,13 @@ public:
         dev_.Abig = d_Abig_;
         cuda_check(cudaFuncSetAttribute((const void *)mf::k_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kUpdateSmem), "cudaFuncSetAttribute");
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kPanelSmem), "cudaFuncSetAttribute");
         cuda_check(cudaFuncSetAttribute((const void *)mf::k_panel_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kPairSmem), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_inverse_row, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_xinv_gemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kPairSmem), "cudaFuncSetAttribute");
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_xinv_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kPairSmem), "cudaFuncSetAttribute");
         if (small_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the solve kernels' shared-memory window");
         cuda_check(cudaFuncSetAttribute((const void *)mf::k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_smem_), "cudaFuncSetAttribute");
@@ -696,20 +788,20 @@ public:
                     maxt = std::max(maxt, nti * (nti + 1) / 2);
                     maxr = std::max(maxr, (nt + mf::PW - 1) / mf::PW);
                 }
-                mf::k_panel<<<cnt, 256, 0, st>>>(dev_, d_lvl_.p + q0, k0, d_err_);
+                mf::k_panel<<<cnt, 256, kPanelSmem, st>>>(dev_, d_lvl_.p + q0, k0, d_err_);
                 if (maxr > 0) mf::k_panel_trsm<<<dim3(maxr, cnt), 256, kPairSmem, st>>>(dev_, d_lvl_.p + q0, k0);
                 if (maxt > 0) {
                     dim3 grid(std::min(maxt, 4096), cnt);
                     mf::k_update<<<grid, 256, kUpdateSmem, st>>>(dev_, d_lvl_.p + q0, k0);
                 }
             }
-            int b0 = big_start_[l], b1 = big_start_[l + 1];
-            if (b1 > b0) {
-                int nbmax = (S.ncol[big_list_[b0]] + mf::PW - 1) / mf::PW;
-                for (int bi = 0; bi < nbmax; bi++) {
-                    int cnt = 0;
-                    while (b0 + cnt < b1 && (S.ncol[big_list_[b0 + cnt]] + mf::PW - 1) / mf::PW > bi) cnt++;
-                    mf::k_inverse_row<<<dim3(bi + 1, cnt), 256, kPairSmem, st>>>(dev_, d_big_.p + b0, bi);
+            for (int pass = xinv_pass_start_[l]; pass < xinv_pass_start_[l + 1]; pass++) {
+                int t0 = xinv_task_start_[pass], nt = xinv_task_start_[pass + 1] - t0;
+                const int4 *tk = d_xinv_tasks_.p + t0;
+                switch (xinv_pass_kind_[pass]) {
+                case 0: mf::k_xinv_diag<<<nt, 256, 0, st>>>(dev_, tk); break;
+                case 1: mf::k_xinv_gemm<0><<<nt, 256, kPairSmem, st>>>(dev_, tk); break;
+                default: mf::k_xinv_gemm<1><<<nt, 256, kPairSmem, st>>>(dev_, tk); break;
                 }
             }
         }
@@ -760,8 +852,8 @@ public:
                     mnr = std::max(mnr, S.m[big_list_[q]] - S.ncol[big_list_[q]]);
                 }
                 mf::k_wide_fwd_acc<<<bc, 512, 0, st>>>(dev_, d_big_.p + b0, d_y_);
-                mf::k_wide_fwd_y<<<dim3((mnc + 31) / 32, bc), 256, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
-                mf::k_wide_fwd_t<<<dim3((mnr + 31) / 32, bc), 256, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
+                mf::k_wide_fwd_y<<<dim3((mnc + mf::RT - 1) / mf::RT, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
+                mf::k_wide_fwd_t<<<dim3((mnr + mf::RT - 1) / mf::RT, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
             }
         }
         for (int l = S.nlevels - 1; l >= 0; l--) {
@@ -770,8 +862,8 @@ public:
             int b0 = big_start_[l], bc = big_start_[l + 1] - b0;
             if (bc > 0) {
                 int mnc = S.ncol[big_list_[b0]];
-                mf::k_wide_bwd_z<<<dim3((mnc + 7) / 8, bc), 256, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_z_);
-                mf::k_wide_bwd_x<<<dim3((mnc + 7) / 8, bc), 256, 0, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
+                mf::k_wide_bwd_z<<<dim3((mnc + 15) / 16, bc), 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_y_, d_z_);
+                mf::k_wide_bwd_x<<<dim3((mnc + 15) / 16, bc), 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
             }
         }
     }
@@ -803,11 +895,14 @@ private:
     const double *factor_vals_ = nullptr;
     static constexpr size_t kUpdateSmem = 2 * mf::UT * (mf::PW + 1) * sizeof(double);
     static constexpr size_t kPairSmem = 2 * mf::PW * (mf::PW + 1) * sizeof(double);
+    static constexpr size_t kPanelSmem = kPairSmem + 32 * 33 * sizeof(double);
     cudaStream_t st_;
     cusolverSpHandle_t hsp_ = nullptr;
     std::vector<int64_t> inv_off_, xinv_off_;
     std::vector<int32_t> small_start_, small_list_, big_start_, big_list_;
-    size_t small_smem_ = 8;
+    std::vector<int> xinv_pass_start_, xinv_task_start_, xinv_pass_kind_;
+    DBuf<int4> d_xinv_tasks_;
+    size_t small_smem_ = 8, wide_smem_ = 8;
     DBuf<int64_t> d_inv_off_, d_xinv_off_;
     DBuf<int32_t> d_small_, d_big_;
     DBuf<double> d_Inv_, d_Xinv_, d_Abig_, d_y1_, d_z_;
