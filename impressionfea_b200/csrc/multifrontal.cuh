@@ -28,33 +28,36 @@ namespace mf {
 constexpr int PW = 64;  // panel width
 constexpr int UT = 64;  // update tile
 
+template <typename T>
 struct Dev {
     const int32_t *ncol, *m, *c0, *idx_start, *idx, *relmap_start, *relmap, *uvec_start, *child_start, *child_list;
     const int64_t *front_off, *inv_off, *xinv_off;
-    double *F, *U, *Inv, *Xinv, *Abig;
+    T *F, *U, *Inv, *Xinv, *Abig;
 };
 
 constexpr int kWideM = 192;  // fronts at least this tall get a full pivot-block inverse and multi-CTA solves
 
+template <typename T>
 static __global__ void k_scatter(int64_t n, const int64_t *__restrict__ dst, const int32_t *__restrict__ src,
-                          const double *__restrict__ vals, double *__restrict__ F)
+                          const double *__restrict__ vals, T *__restrict__ F)
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-        F[dst[t]] = vals[src[t]];
+        F[dst[t]] = (T)vals[src[t]];
 }
 
 // Extend-add of the update matrices of the listed children into their parents' fronts.
-static __global__ void k_extend(Dev D, const int32_t *__restrict__ children, const int32_t *__restrict__ parents)
+template <typename T>
+static __global__ void k_extend(Dev<T> D, const int32_t *__restrict__ children, const int32_t *__restrict__ parents)
 {
     int c = children[blockIdx.y];
     int p = parents[c];
     int mc = D.m[c], nc = D.ncol[c], nr = mc - nc, mp = D.m[p];
-    const double *Fc = D.F + D.front_off[c];
-    double *Fp = D.F + D.front_off[p];
+    const T *Fc = D.F + D.front_off[c];
+    T *Fp = D.F + D.front_off[p];
     const int32_t *rm = D.relmap + D.relmap_start[c];
     for (int j = blockIdx.x; j < nr; j += gridDim.x) {
         int64_t pj = (int64_t)rm[j] * mp;
-        const double *col = Fc + (int64_t)(nc + j) * mc + nc;
+        const T *col = Fc + (int64_t)(nc + j) * mc + nc;
         for (int i = j + threadIdx.x; i < nr; i += blockDim.x) Fp[pj + rm[i]] += col[i];
     }
 }
@@ -65,34 +68,36 @@ static __global__ void k_extend(Dev D, const int32_t *__restrict__ children, con
 // identity. The inverse is built by recursive doubling: the 8x8 diagonal blocks are inverted by forward
 // substitution in registers, then pairs of blocks merge with X21 = -X22 L21 X11 at sizes 8, 16 and 32. The lowest
 // failing pivot column (new numbering) goes to err. Dynamic shared memory: two 64 x 65 blocks and a 32 x 33 one.
-static __global__ void __launch_bounds__(256) k_panel(Dev D, const int32_t *__restrict__ fronts, int k0, int *err)
+template <typename T>
+static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *__restrict__ fronts, int k0, int *err)
 {
-    extern __shared__ double shp[];
-    double (*Ds)[PW + 1] = (double (*)[PW + 1])shp;
-    double (*Xs)[PW + 1] = (double (*)[PW + 1])(shp + PW * (PW + 1));
-    double (*Ts)[33] = (double (*)[33])(shp + 2 * PW * (PW + 1));
-    __shared__ double sq[PW];
+    extern __shared__ __align__(16) unsigned char shp_raw[];
+    T *shp = (T *)shp_raw;
+    T (*Ds)[PW + 1] = (T (*)[PW + 1])shp;
+    T (*Xs)[PW + 1] = (T (*)[PW + 1])(shp + PW * (PW + 1));
+    T (*Ts)[33] = (T (*)[33])(shp + 2 * PW * (PW + 1));
+    __shared__ T sq[PW];
     int s = fronts[blockIdx.x];
     int ms = D.m[s], w = min(PW, D.ncol[s] - k0);
-    double *F = D.F + D.front_off[s];
-    double *Inv = D.Inv + D.inv_off[s] + (int64_t)(k0 / PW) * PW * PW;
+    T *F = D.F + D.front_off[s];
+    T *Inv = D.Inv + D.inv_off[s] + (int64_t)(k0 / PW) * PW * PW;
     int tid = threadIdx.x, r = tid & (PW - 1), cg = tid >> 6;
     for (int t = tid; t < PW * PW; t += blockDim.x) {
         int rr = t % PW, c = t / PW;
-        double v = rr == c ? 1.0 : 0.0;
+        T v = rr == c ? 1.0 : 0.0;
         if (rr < w && c < w && rr >= c) v = F[(int64_t)(k0 + c) * ms + k0 + rr];
         Ds[rr][c] = v;
         Xs[rr][c] = 0.0;
     }
     __syncthreads();
     for (int k = 0; k < w; k++) {
-        double d = Ds[k][k];
+        T d = Ds[k][k];
         if (!(d > 0)) {
             if (tid == 0) atomicMin(err, D.c0[s] + k0 + k);
             return;  // every thread read the same pivot: a uniform exit
         }
         if (r > k) {
-            double a = Ds[r][k] / d;
+            T a = Ds[r][k] / d;
             for (int c = k + 1 + cg; c <= r; c += 4) Ds[r][c] -= a * Ds[c][k];
         }
         __syncthreads();
@@ -108,10 +113,10 @@ static __global__ void __launch_bounds__(256) k_panel(Dev D, const int32_t *__re
     // 8x8 diagonal blocks: thread (b, j) forward-substitutes column j of block b
     if (tid < PW) {
         int b8 = (tid >> 3) * 8, j = tid & 7;
-        double x[8];
+        T x[8];
 #pragma unroll
         for (int i = 0; i < 8; i++) {
-            double v = i == j ? 1.0 : 0.0;
+            T v = i == j ? 1.0 : 0.0;
 #pragma unroll
             for (int q = 0; q < i; q++) v -= Ds[b8 + i][b8 + q] * x[q];
             x[i] = v / Ds[b8 + i][b8 + i];
@@ -125,14 +130,14 @@ static __global__ void __launch_bounds__(256) k_panel(Dev D, const int32_t *__re
         int per = h * h, total = (PW / (2 * h)) * per;
         for (int t = tid; t < total; t += blockDim.x) {
             int p = t / per, e = t % per, i = e / h, j = e % h, b = p * 2 * h;
-            double v = 0;
+            T v = 0;
             for (int q = j; q < h; q++) v += Ds[b + h + i][b + q] * Xs[b + q][b + j];
             Ts[p * h + i][j] = v;  // the pairs of one size fill 32 rows
         }
         __syncthreads();
         for (int t = tid; t < total; t += blockDim.x) {
             int p = t / per, e = t % per, i = e / h, j = e % h, b = p * 2 * h;
-            double v = 0;
+            T v = 0;
             for (int q = 0; q <= i; q++) v += Xs[b + h + i][b + h + q] * Ts[p * h + q][j];
             Xs[b + h + i][b + j] = -v;
         }
@@ -146,18 +151,20 @@ static __global__ void __launch_bounds__(256) k_panel(Dev D, const int32_t *__re
 
 // Rows below the diagonal block of panel k0, 64 rows per CTA: X = F21 L11^-T = F21 Dinv^T, i.e.
 // x_k = sum_{l<=k} f_l Dinv[k][l], with Dinv the stored inverse of the diagonal block.
-static __global__ void __launch_bounds__(256) k_panel_trsm(Dev D, const int32_t *__restrict__ fronts, int k0)
+template <typename T>
+static __global__ void __launch_bounds__(256) k_panel_trsm(Dev<T> D, const int32_t *__restrict__ fronts, int k0)
 {
-    extern __shared__ double shm[];
-    double (*Di)[PW + 1] = (double (*)[PW + 1])shm;
-    double (*Ft)[PW + 1] = (double (*)[PW + 1])(shm + PW * (PW + 1));
+    extern __shared__ __align__(16) unsigned char shm_raw[];
+    T *shm = (T *)shm_raw;
+    T (*Di)[PW + 1] = (T (*)[PW + 1])shm;
+    T (*Ft)[PW + 1] = (T (*)[PW + 1])(shm + PW * (PW + 1));
     int s = fronts[blockIdx.y];
     int ms = D.m[s], w = min(PW, D.ncol[s] - k0);
     int rbeg = k0 + w + blockIdx.x * PW;
     if (rbeg >= ms) return;
     int rows = min(PW, ms - rbeg);
-    double *F = D.F + D.front_off[s];
-    const double *Inv = D.Inv + D.inv_off[s] + (int64_t)(k0 / PW) * PW * PW;
+    T *F = D.F + D.front_off[s];
+    const T *Inv = D.Inv + D.inv_off[s] + (int64_t)(k0 / PW) * PW * PW;
     for (int t = threadIdx.x; t < PW * PW; t += blockDim.x) {
         int c = t / PW, i = t % PW;
         Di[i][c] = Inv[t];  // column-major inverse: row i, column c
@@ -168,11 +175,11 @@ static __global__ void __launch_bounds__(256) k_panel_trsm(Dev D, const int32_t 
     }
     __syncthreads();
     int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double acc[4][4];
+    T acc[4][4];
     for (int a = 0; a < 4; a++)
         for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
     for (int l = 0; l < w; l++) {
-        double f[4], d[4];
+        T f[4], d[4];
         for (int a = 0; a < 4; a++) f[a] = Ft[tx + 16 * a][l];
         for (int b = 0; b < 4; b++) d[b] = Di[ty + 16 * b][l];
         for (int a = 0; a < 4; a++)
@@ -191,33 +198,35 @@ static __global__ void __launch_bounds__(256) k_panel_trsm(Dev D, const int32_t 
 // 64 x 64 output tiles (bi in the bottom half, bj in the top half): T = L21 X11 (k_xinv_gemm<0>, stored transposed
 // in X's unused upper triangle), then X21 = -X22 T (k_xinv_gemm<1>). The tasks (front, bi, bj, gm) of one pass are
 // listed on the host; one CTA per task, each thread a 4 x 4 register block.
-static __global__ void k_xinv_diag(Dev D, const int4 *__restrict__ tasks)
+template <typename T>
+static __global__ void k_xinv_diag(Dev<T> D, const int4 *__restrict__ tasks)
 {
     int4 tk = tasks[blockIdx.x];
     int s = tk.x, bi = tk.y, nc = D.ncol[s], r0 = bi * PW, w = min(PW, nc - r0);
-    const double *Dinv = D.Inv + D.inv_off[s] + (int64_t)bi * PW * PW;
-    double *X = D.Xinv + D.xinv_off[s];
+    const T *Dinv = D.Inv + D.inv_off[s] + (int64_t)bi * PW * PW;
+    T *X = D.Xinv + D.xinv_off[s];
     for (int t = threadIdx.x; t < PW * PW; t += blockDim.x) {
         int c = t / PW, r = t % PW;
         if (r < w && c < w) X[(int64_t)(r0 + c) * nc + r0 + r] = Dinv[t];
     }
 }
 
-template <int PASS>
-static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev D, const int4 *__restrict__ tasks)
+template <typename T, int PASS>
+static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev<T> D, const int4 *__restrict__ tasks)
 {
-    extern __shared__ double shm[];
-    double (*A)[PW + 1] = (double (*)[PW + 1])shm;
-    double (*B)[PW + 1] = (double (*)[PW + 1])(shm + PW * (PW + 1));
+    extern __shared__ __align__(16) unsigned char shm_raw[];
+    T *shm = (T *)shm_raw;
+    T (*A)[PW + 1] = (T (*)[PW + 1])shm;
+    T (*B)[PW + 1] = (T (*)[PW + 1])(shm + PW * (PW + 1));
     int4 tk = tasks[blockIdx.x];
     int s = tk.x, bi = tk.y, bj = tk.z, gm = tk.w;
     int ms = D.m[s], nc = D.ncol[s];
-    const double *F = D.F + D.front_off[s];
-    double *X = D.Xinv + D.xinv_off[s];
+    const T *F = D.F + D.front_off[s];
+    T *X = D.Xinv + D.xinv_off[s];
     int r0 = bi * PW, c0 = bj * PW, wr = min(PW, nc - r0), wc = min(PW, nc - c0);
     int kb0 = PASS == 0 ? bj : gm, kb1 = PASS == 0 ? gm : bi + 1;
     int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double acc[4][4];
+    T acc[4][4];
     for (int a = 0; a < 4; a++)
         for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
     for (int bk = kb0; bk < kb1; bk++) {
@@ -237,7 +246,7 @@ static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev D, const int4 *__r
         }
         __syncthreads();
         for (int k = 0; k < PW; k++) {
-            double a4[4], b4[4];
+            T a4[4], b4[4];
             for (int a = 0; a < 4; a++) a4[a] = A[tx + 16 * a][k];
             for (int b = 0; b < 4; b++) b4[b] = B[k][ty + 16 * b];
             for (int a = 0; a < 4; a++)
@@ -259,18 +268,19 @@ static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev D, const int4 *__r
 // Per-front scratch vectors live at offset idx_start[s] (length m) in Abig (assembled right-hand side), Y1, Z.
 
 // acc = [b(cols); 0] - children's update vectors (in child order).
-static __global__ void k_wide_fwd_acc(Dev D, const int32_t *__restrict__ fronts, const double *y)
+template <typename T>
+static __global__ void k_wide_fwd_acc(Dev<T> D, const int32_t *__restrict__ fronts, const T *y)
 {
     int s = fronts[blockIdx.x];
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s];
-    double *acc = D.Abig + D.idx_start[s];
+    T *acc = D.Abig + D.idx_start[s];
     for (int k = threadIdx.x; k < ms; k += blockDim.x) acc[k] = k < nc ? y[c0 + k] : 0.0;
     __syncthreads();
     for (int q = D.child_start[s]; q < D.child_start[s + 1]; q++) {
         int c = D.child_list[q];
         int nr = D.m[c] - D.ncol[c];
         const int32_t *rm = D.relmap + D.relmap_start[c];
-        const double *u = D.U + D.uvec_start[c];
+        const T *u = D.U + D.uvec_start[c];
         for (int i = threadIdx.x; i < nr; i += blockDim.x) acc[rm[i]] -= u[i];
         __syncthreads();
     }
@@ -283,18 +293,19 @@ static __global__ void k_wide_fwd_acc(Dev D, const int32_t *__restrict__ fronts,
 constexpr int RT = 16;
 
 // y1 = X acc1 (X lower triangular).
-static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev D, const int32_t *__restrict__ fronts, double *y, double *Y1)
+template <typename T>
+static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32_t *__restrict__ fronts, T *y, T *Y1)
 {
-    __shared__ double part[32][RT + 1];
+    __shared__ T part[32][RT + 1];
     int s = fronts[blockIdx.y];
     int nc = D.ncol[s], c0 = D.c0[s], ntile = (nc + RT - 1) / RT;
     if ((int)blockIdx.x >= ntile) return;
     int r0 = (ntile - 1 - blockIdx.x) * RT;
-    const double *X = D.Xinv + D.xinv_off[s];
-    const double *acc = D.Abig + D.idx_start[s];
+    const T *X = D.Xinv + D.xinv_off[s];
+    const T *acc = D.Abig + D.idx_start[s];
     int lane = threadIdx.x & 31, sub = (lane >> 4) + 2 * (threadIdx.x >> 5), rr = lane & (RT - 1);
     int r = r0 + rr, cend = min(nc, r0 + RT);
-    double v = 0;
+    T v = 0;
     if (r < nc) {
 #pragma unroll 8
         for (int c = sub; c < cend; c += 32)
@@ -303,7 +314,7 @@ static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev D, const int32_t 
     part[sub][rr] = v;
     __syncthreads();
     if (threadIdx.x < RT && r0 + (int)threadIdx.x < nc) {
-        double t = 0;
+        T t = 0;
         for (int q = 0; q < 32; q++) t += part[q][threadIdx.x];
         y[c0 + r0 + threadIdx.x] = t;
         Y1[D.idx_start[s] + r0 + threadIdx.x] = t;
@@ -311,18 +322,19 @@ static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev D, const int32_t 
 }
 
 // update vector t = -acc2 + L21 y1.
-static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev D, const int32_t *__restrict__ fronts, const double *Y1)
+template <typename T>
+static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32_t *__restrict__ fronts, const T *Y1)
 {
-    __shared__ double part[32][RT + 1];
+    __shared__ T part[32][RT + 1];
     int s = fronts[blockIdx.y];
     int ms = D.m[s], nc = D.ncol[s], nr = ms - nc;
     int i0 = blockIdx.x * RT;
     if (i0 >= nr) return;
-    const double *F = D.F + D.front_off[s] + nc;
-    const double *y1 = Y1 + D.idx_start[s];
+    const T *F = D.F + D.front_off[s] + nc;
+    const T *y1 = Y1 + D.idx_start[s];
     int lane = threadIdx.x & 31, sub = (lane >> 4) + 2 * (threadIdx.x >> 5), rr = lane & (RT - 1);
     int i = i0 + rr;
-    double v = 0;
+    T v = 0;
     if (i < nr) {
 #pragma unroll 8
         for (int k = sub; k < nc; k += 32) v += F[(int64_t)k * ms + i] * y1[k];
@@ -330,7 +342,7 @@ static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev D, const int32_t 
     part[sub][rr] = v;
     __syncthreads();
     if (threadIdx.x < RT && i0 + (int)threadIdx.x < nr) {
-        double t = 0;
+        T t = 0;
         for (int q = 0; q < 32; q++) t += part[q][threadIdx.x];
         int ii = i0 + threadIdx.x;
         D.U[D.uvec_start[s] + ii] = -D.Abig[D.idx_start[s] + nc + ii] + t;
@@ -338,9 +350,11 @@ static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev D, const int32_t 
 }
 
 // z = y1 - L21^T x2, one warp per pivot column; x2 is gathered into shared memory once per CTA.
-static __global__ void __launch_bounds__(512) k_wide_bwd_z(Dev D, const int32_t *__restrict__ fronts, const double *x, double *Z)
+template <typename T>
+static __global__ void __launch_bounds__(512) k_wide_bwd_z(Dev<T> D, const int32_t *__restrict__ fronts, const T *x, T *Z)
 {
-    extern __shared__ double xs[];
+    extern __shared__ __align__(16) unsigned char xs_raw[];
+    T *xs = (T *)xs_raw;
     int s = fronts[blockIdx.y];
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s], nr = ms - nc;
     int kbase = blockIdx.x * (blockDim.x >> 5);
@@ -350,9 +364,9 @@ static __global__ void __launch_bounds__(512) k_wide_bwd_z(Dev D, const int32_t 
     __syncthreads();
     int k = kbase + (threadIdx.x >> 5);
     if (k >= nc) return;
-    const double *col = D.F + D.front_off[s] + (int64_t)k * ms + nc;
+    const T *col = D.F + D.front_off[s] + (int64_t)k * ms + nc;
     int lane = threadIdx.x & 31;
-    double v = 0;
+    T v = 0;
 #pragma unroll 8
     for (int i = lane; i < nr; i += 32) v += col[i] * xs[i];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -360,22 +374,24 @@ static __global__ void __launch_bounds__(512) k_wide_bwd_z(Dev D, const int32_t 
 }
 
 // x1 = X^T z, one warp per pivot column j (column j of X is contiguous); z is staged in shared memory.
-static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev D, const int32_t *__restrict__ fronts, const double *Z, double *x)
+template <typename T>
+static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev<T> D, const int32_t *__restrict__ fronts, const T *Z, T *x)
 {
-    extern __shared__ double zs[];
+    extern __shared__ __align__(16) unsigned char zs_raw[];
+    T *zs = (T *)zs_raw;
     int s = fronts[blockIdx.y];
     int nc = D.ncol[s], c0 = D.c0[s];
     int nw = blockDim.x >> 5, nblk = (nc + nw - 1) / nw;
     if ((int)blockIdx.x >= nblk) return;
     int jbase = (nblk - 1 - blockIdx.x) * nw;  // leftmost (longest) columns first
-    const double *z = Z + D.idx_start[s];
+    const T *z = Z + D.idx_start[s];
     for (int i = jbase + threadIdx.x; i < nc; i += blockDim.x) zs[i - jbase] = z[i];
     __syncthreads();
     int j = jbase + (threadIdx.x >> 5);
     if (j >= nc) return;
-    const double *col = D.Xinv + D.xinv_off[s] + (int64_t)j * nc;
+    const T *col = D.Xinv + D.xinv_off[s] + (int64_t)j * nc;
     int lane = threadIdx.x & 31;
-    double v = 0;
+    T v = 0;
 #pragma unroll 8
     for (int i = j + lane; i < nc; i += 32) v += col[i] * zs[i - jbase];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -384,15 +400,17 @@ static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev D, const int32_t 
 
 // Trailing update of every listed front after panel k0: F22 -= L21 L21^T on 64x64 lower tiles, each thread a
 // 4x4 register block (dynamic shared memory: two 64 x PW panels).
-static __global__ void __launch_bounds__(256) k_update(Dev D, const int32_t *__restrict__ fronts, int k0)
+template <typename T>
+static __global__ void __launch_bounds__(256) k_update(Dev<T> D, const int32_t *__restrict__ fronts, int k0)
 {
-    extern __shared__ double sh[];
-    double (*Ai)[PW + 1] = (double (*)[PW + 1])sh;
-    double (*Aj)[PW + 1] = (double (*)[PW + 1])(sh + UT * (PW + 1));
+    extern __shared__ __align__(16) unsigned char sh_raw[];
+    T *sh = (T *)sh_raw;
+    T (*Ai)[PW + 1] = (T (*)[PW + 1])sh;
+    T (*Aj)[PW + 1] = (T (*)[PW + 1])(sh + UT * (PW + 1));
     int s = fronts[blockIdx.y];
     int ms = D.m[s], w = min(PW, D.ncol[s] - k0), r0 = k0 + w, nt = ms - r0;
     if (nt <= 0) return;
-    double *F = D.F + D.front_off[s];
+    T *F = D.F + D.front_off[s];
     int nti = (nt + UT - 1) / UT;
     int ntiles = nti * (nti + 1) / 2;
     int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -410,11 +428,11 @@ static __global__ void __launch_bounds__(256) k_update(Dev D, const int32_t *__r
             Aj[rr][k] = gj < ms ? F[(int64_t)(k0 + k) * ms + gj] : 0.0;
         }
         __syncthreads();
-        double acc[4][4];
+        T acc[4][4];
         for (int a = 0; a < 4; a++)
             for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
         for (int k = 0; k < w; k++) {
-            double ai[4], aj[4];
+            T ai[4], aj[4];
             for (int a = 0; a < 4; a++) ai[a] = Ai[tx + 16 * a][k];
             for (int b = 0; b < 4; b++) aj[b] = Aj[ty + 16 * b][k];
             for (int a = 0; a < 4; a++)
@@ -434,25 +452,29 @@ static __global__ void k_init_err(int *err)
     err[1] = 0;
 }
 
-static __global__ void k_permute_in(int n, const int32_t *perm, const double *b, double *y)
+template <typename T>
+static __global__ void k_permute_in(int n, const int32_t *perm, const double *b, T *y)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = b[perm[i]];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = (T)b[perm[i]];
 }
-static __global__ void k_permute_out(int n, const int32_t *perm, const double *y, double *x)
+template <typename T>
+static __global__ void k_permute_out(int n, const int32_t *perm, const T *y, double *x)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[perm[i]] = y[i];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[perm[i]] = (double)y[i];
 }
 
 // Forward elimination of the fronts of one level: y(cols) and the update vector for the parent. Each 64-pivot
 // block is applied through its stored inverse (one block GEMV) instead of 64 dependent steps.
-static __global__ void __launch_bounds__(512) k_forward(Dev D, const int32_t *__restrict__ fronts, double *y)
+template <typename T>
+static __global__ void __launch_bounds__(512) k_forward(Dev<T> D, const int32_t *__restrict__ fronts, T *y)
 {
-    extern __shared__ double acc[];
-    __shared__ double yb[PW];
+    extern __shared__ __align__(16) unsigned char acc_raw[];
+    T *acc = (T *)acc_raw;
+    __shared__ T yb[PW];
     int s = fronts[blockIdx.x];
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s];
-    const double *F = D.F + D.front_off[s];
-    const double *Inv = D.Inv + D.inv_off[s];
+    const T *F = D.F + D.front_off[s];
+    const T *Inv = D.Inv + D.inv_off[s];
     int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     for (int k = tid; k < ms; k += nt) acc[k] = k < nc ? y[c0 + k] : 0.0;
     __syncthreads();
@@ -460,16 +482,16 @@ static __global__ void __launch_bounds__(512) k_forward(Dev D, const int32_t *__
         int c = D.child_list[q];
         int nr = D.m[c] - D.ncol[c];
         const int32_t *rm = D.relmap + D.relmap_start[c];
-        const double *u = D.U + D.uvec_start[c];
+        const T *u = D.U + D.uvec_start[c];
         for (int i = tid; i < nr; i += nt) acc[rm[i]] -= u[i];
         __syncthreads();
     }
     for (int kb = 0; kb < nc; kb += PW) {
         int w = min(PW, nc - kb);
-        const double *I = Inv + (int64_t)(kb / PW) * PW * PW;
+        const T *I = Inv + (int64_t)(kb / PW) * PW * PW;
         // y_blk = Linv acc_blk (warp per output row, coalesced over the inverse's columns? rows: I[c*PW + i])
         for (int i = warp; i < w; i += nw) {
-            double v = 0;
+            T v = 0;
             for (int c = lane; c <= i; c += 32) v += I[(int64_t)c * PW + i] * acc[kb + c];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) yb[i] = v;
@@ -478,35 +500,37 @@ static __global__ void __launch_bounds__(512) k_forward(Dev D, const int32_t *__
         for (int i = tid; i < w; i += nt) acc[kb + i] = yb[i];
         // rows below the block
         for (int r = kb + w + tid; r < ms; r += nt) {
-            double v = acc[r];
+            T v = acc[r];
             for (int k = 0; k < w; k++) v -= F[(int64_t)(kb + k) * ms + r] * yb[k];
             acc[r] = v;
         }
         __syncthreads();
     }
     for (int k = tid; k < nc; k += nt) y[c0 + k] = acc[k];
-    double *u = D.U + D.uvec_start[s];
+    T *u = D.U + D.uvec_start[s];
     for (int i = tid; i < ms - nc; i += nt) u[i] = -acc[nc + i];
 }
 
 // Back substitution of the fronts of one level: x(cols) from y(cols) and the solved ancestors' x.
-static __global__ void __launch_bounds__(512) k_backward(Dev D, const int32_t *__restrict__ fronts, const double *y, double *x)
+template <typename T>
+static __global__ void __launch_bounds__(512) k_backward(Dev<T> D, const int32_t *__restrict__ fronts, const T *y, T *x)
 {
-    extern __shared__ double sm[];
-    __shared__ double xb[PW];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T *sm = (T *)sm_raw;
+    __shared__ T xb[PW];
     int s = fronts[blockIdx.x];
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s], nr = ms - nc;
-    const double *F = D.F + D.front_off[s];
-    const double *Inv = D.Inv + D.inv_off[s];
+    const T *F = D.F + D.front_off[s];
+    const T *Inv = D.Inv + D.inv_off[s];
     const int32_t *ix = D.idx + D.idx_start[s];
-    double *acc = sm, *xs = sm + nc;
+    T *acc = sm, *xs = sm + nc;
     int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     for (int k = tid; k < nc; k += nt) acc[k] = y[c0 + k];
     for (int i = tid; i < nr; i += nt) xs[i] = x[ix[nc + i]];
     __syncthreads();
     for (int k = warp; k < nc; k += nw) {
-        const double *col = F + (int64_t)k * ms + nc;
-        double v = 0;
+        const T *col = F + (int64_t)k * ms + nc;
+        T v = 0;
         for (int i = lane; i < nr; i += 32) v += col[i] * xs[i];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
         if (lane == 0) acc[k] -= v;
@@ -516,17 +540,17 @@ static __global__ void __launch_bounds__(512) k_backward(Dev D, const int32_t *_
     for (int bi = nblk - 1; bi >= 0; bi--) {
         int kb = bi * PW, w = min(PW, nc - kb), ke = kb + w;
         for (int j = kb + warp; j < ke; j += nw) {
-            const double *col = F + (int64_t)j * ms;
-            double v = 0;
+            const T *col = F + (int64_t)j * ms;
+            T v = 0;
             for (int k = ke + lane; k < nc; k += 32) v += col[k] * acc[k];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) acc[j] -= v;
         }
         __syncthreads();
         // x_blk = Linv^T acc_blk: x_j = sum_{i >= j} Linv[i][j] acc_i (column j of the inverse is contiguous)
-        const double *I = Inv + (int64_t)bi * PW * PW;
+        const T *I = Inv + (int64_t)bi * PW * PW;
         for (int j = warp; j < w; j += nw) {
-            double v = 0;
+            T v = 0;
             for (int i = j + lane; i < w; i += 32) v += I[(int64_t)j * PW + i] * acc[kb + i];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) xb[j] = v;
@@ -546,9 +570,33 @@ static __global__ void k_finite(int n, const double *x, int *flag)
 
 }  // namespace mf
 
-class MfSolver {
+// The linear solver behind the stepper: analyse once per pattern, factorise device values, solve on the device.
+// Implemented by the multifrontal Cholesky in double precision (the drop-in) and in single precision (the factor
+// that FP64 conjugate-gradient refinement uses as its preconditioner).
+class LinearSolver {
 public:
-    explicit MfSolver(cudaStream_t s) : st_(s)
+    virtual ~LinearSolver() = default;
+    virtual void set_stream(cudaStream_t s) = 0;
+    virtual void analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block) = 0;
+    virtual void factorize(const double *d_full_vals) = 0;
+    virtual void solve(const double *d_b, double *d_x) = 0;
+    virtual void check_finite(const double *d_x) = 0;
+    virtual const MfSymbolic &symbolic() const = 0;
+    virtual int64_t factor_nonzeros() const = 0;
+    virtual int big_fronts() const = 0;
+    virtual double factor_ms() const = 0;
+    virtual double solve_ms() const = 0;
+    virtual int64_t solves() const = 0;
+    virtual void set_profile(bool p) = 0;
+    virtual bool analyzed() const = 0;
+    virtual bool factored() const = 0;
+    virtual int value_bytes() const = 0;
+};
+
+template <typename T>
+class MfSolverT final : public LinearSolver {
+public:
+    explicit MfSolverT(cudaStream_t s) : st_(s)
     {
         if (cusolverSpCreate(&hsp_) != CUSOLVER_STATUS_SUCCESS) throw Failure(IFEA_CUDA_ERROR, "cusolverSpCreate failed");
         if (cusparseCreateMatDescr(&descr_) != CUSPARSE_STATUS_SUCCESS) throw Failure(IFEA_CUDA_ERROR, "cusparseCreateMatDescr failed");
@@ -558,7 +606,7 @@ public:
         cuda_check(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking), "cudaStreamCreate");
         for (auto &e : ev_) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
     }
-    ~MfSolver()
+    ~MfSolverT() override
     {
         drop_graphs();
         for (auto &e : ev_)
@@ -567,22 +615,23 @@ public:
         if (descr_) cusparseDestroyMatDescr(descr_);
         if (hsp_) cusolverSpDestroy(hsp_);
     }
-    MfSolver(const MfSolver &) = delete;
-    MfSolver &operator=(const MfSolver &) = delete;
+    MfSolverT(const MfSolverT &) = delete;
+    MfSolverT &operator=(const MfSolverT &) = delete;
 
-    void set_stream(cudaStream_t s) { st_ = s; }
-    bool analyzed() const { return analyzed_; }
-    bool factored() const { return factored_; }
-    int64_t factor_nonzeros() const { return sym_.factor_nnz; }
-    const MfSymbolic &symbolic() const { return sym_; }
-    int big_fronts() const { return (int)big_list_.size(); }
-    double factor_ms() const { return factor_ms_; }
-    double solve_ms() const { return solve_ms_; }
-    int64_t solves() const { return n_solves_; }
-    void set_profile(bool p) { profile_ = p; }
+    void set_stream(cudaStream_t s) override { st_ = s; }
+    bool analyzed() const override { return analyzed_; }
+    bool factored() const override { return factored_; }
+    int64_t factor_nonzeros() const override { return sym_.factor_nnz; }
+    const MfSymbolic &symbolic() const override { return sym_; }
+    int big_fronts() const override { return (int)big_list_.size(); }
+    double factor_ms() const override { return factor_ms_; }
+    double solve_ms() const override { return solve_ms_; }
+    int64_t solves() const override { return n_solves_; }
+    int value_bytes() const override { return (int)sizeof(T); }
+    void set_profile(bool p) override { profile_ = p; }
     int n() const { return sym_.n; }
 
-    void analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block)
+    void analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block) override
     {
         analyzed_ = factored_ = false;
         drop_graphs();
@@ -652,10 +701,10 @@ public:
                              [&](int a, int b) { return S.ncol[a] > S.ncol[b]; });
         d_big_.upload(big_list_, st_);
         wide_smem_ = 8;
-        for (int sn : big_list_) wide_smem_ = std::max(wide_smem_, (size_t)std::max(S.ncol[sn], S.m[sn] - S.ncol[sn]) * sizeof(double));
+        for (int sn : big_list_) wide_smem_ = std::max(wide_smem_, (size_t)std::max(S.ncol[sn], S.m[sn] - S.ncol[sn]) * sizeof(T));
         if (wide_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the wide solve kernels' shared-memory window");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_wide_bwd_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wide_smem_), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_wide_bwd_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wide_smem_), "cudaFuncSetAttribute");
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_wide_bwd_z<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wide_smem_), "cudaFuncSetAttribute");
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_wide_bwd_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wide_smem_), "cudaFuncSetAttribute");
         // inverse passes of the wide supernodes, per level: diagonal copies, then for groups of 2, 4, ... blocks
         // the T pass and the X21 pass
         std::vector<int4> tasks;
@@ -697,7 +746,7 @@ public:
         d_Abig_.resize(S.idx_start[S.nsuper]);
         d_y1_.resize(S.idx_start[S.nsuper]);
         d_z_.resize(S.idx_start[S.nsuper]);
-        small_smem_ = (size_t)max_small_m * sizeof(double);
+        small_smem_ = (size_t)max_small_m * sizeof(T);
         d_F_.resize(S.pool);
         d_U_.resize(std::max<int64_t>(S.uvec_pool, 1));
         d_y_.resize(n);
@@ -706,26 +755,26 @@ public:
         dev_.child_list = d_cl_; dev_.front_off = d_off_; dev_.F = d_F_; dev_.U = d_U_;
         dev_.inv_off = d_inv_off_; dev_.Inv = d_Inv_; dev_.xinv_off = d_xinv_off_; dev_.Xinv = d_Xinv_;
         dev_.Abig = d_Abig_;
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kUpdateSmem), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kPanelSmem), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_panel_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_panel_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kPairSmem), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_xinv_gemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_xinv_gemm<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kPairSmem), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_xinv_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_xinv_gemm<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kPairSmem), "cudaFuncSetAttribute");
         if (small_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the solve kernels' shared-memory window");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_smem_), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_smem_), "cudaFuncSetAttribute");
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_forward<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_smem_), "cudaFuncSetAttribute");
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_backward<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_smem_), "cudaFuncSetAttribute");
         cuda_check(cudaStreamSynchronize(st_), "cudaStreamSynchronize");
         analyzed_ = true;
     }
 
     // Numeric factorisation of device values in the order of the analysed full CSC pattern. The launch sequence
     // depends only on the pattern, so it is captured once (per values buffer) as a CUDA graph and replayed.
-    void factorize(const double *d_full_vals)
+    void factorize(const double *d_full_vals) override
     {
         if (!analyzed_) throw Failure(IFEA_BAD_STATE, "Analyze must be called first.");
         factored_ = false;
@@ -764,17 +813,17 @@ public:
         mf::k_init_err<<<1, 1, 0, st>>>(d_err_);
         for (int l = 0; l < S.nlevels; l++) {
             int64_t p0 = S.level_pool_start[l], p1 = S.level_pool_start[l + 1];
-            cuda_check(cudaMemsetAsync(d_F_.p + p0, 0, (size_t)(p1 - p0) * sizeof(double), st), "memset fronts");
+            cuda_check(cudaMemsetAsync(d_F_.p + p0, 0, (size_t)(p1 - p0) * sizeof(T), st), "memset fronts");
             int64_t a0 = S.a_level_start[l], a1 = S.a_level_start[l + 1];
             if (a1 > a0) {
                 int g = (int)std::min<int64_t>((a1 - a0 + 255) / 256, 4 * 148);
-                mf::k_scatter<<<g, 256, 0, st>>>(a1 - a0, d_adst_.p + a0, d_asrc_.p + a0, d_full_vals, d_F_);
+                mf::k_scatter<T><<<g, 256, 0, st>>>(a1 - a0, d_adst_.p + a0, d_asrc_.p + a0, d_full_vals, d_F_);
             }
             for (int r = 0; r < S.max_rank; r++) {
                 int32_t e0 = S.ext_start[(size_t)l * S.max_rank + r], e1 = S.ext_start[(size_t)l * S.max_rank + r + 1];
                 if (e1 <= e0) continue;
                 dim3 grid(64, e1 - e0);
-                mf::k_extend<<<grid, 128, 0, st>>>(dev_, d_ext_.p + e0, d_par_);
+                mf::k_extend<T><<<grid, 128, 0, st>>>(dev_, d_ext_.p + e0, d_par_);
             }
             int q0 = S.level_start[l], q1 = S.level_start[l + 1];
             int maxc = S.ncol[lvl_sorted_[q0]];
@@ -788,20 +837,20 @@ public:
                     maxt = std::max(maxt, nti * (nti + 1) / 2);
                     maxr = std::max(maxr, (nt + mf::PW - 1) / mf::PW);
                 }
-                mf::k_panel<<<cnt, 256, kPanelSmem, st>>>(dev_, d_lvl_.p + q0, k0, d_err_);
-                if (maxr > 0) mf::k_panel_trsm<<<dim3(maxr, cnt), 256, kPairSmem, st>>>(dev_, d_lvl_.p + q0, k0);
+                mf::k_panel<T><<<cnt, 256, kPanelSmem, st>>>(dev_, d_lvl_.p + q0, k0, d_err_);
+                if (maxr > 0) mf::k_panel_trsm<T><<<dim3(maxr, cnt), 256, kPairSmem, st>>>(dev_, d_lvl_.p + q0, k0);
                 if (maxt > 0) {
                     dim3 grid(std::min(maxt, 4096), cnt);
-                    mf::k_update<<<grid, 256, kUpdateSmem, st>>>(dev_, d_lvl_.p + q0, k0);
+                    mf::k_update<T><<<grid, 256, kUpdateSmem, st>>>(dev_, d_lvl_.p + q0, k0);
                 }
             }
             for (int pass = xinv_pass_start_[l]; pass < xinv_pass_start_[l + 1]; pass++) {
                 int t0 = xinv_task_start_[pass], nt = xinv_task_start_[pass + 1] - t0;
                 const int4 *tk = d_xinv_tasks_.p + t0;
                 switch (xinv_pass_kind_[pass]) {
-                case 0: mf::k_xinv_diag<<<nt, 256, 0, st>>>(dev_, tk); break;
-                case 1: mf::k_xinv_gemm<0><<<nt, 256, kPairSmem, st>>>(dev_, tk); break;
-                default: mf::k_xinv_gemm<1><<<nt, 256, kPairSmem, st>>>(dev_, tk); break;
+                case 0: mf::k_xinv_diag<T><<<nt, 256, 0, st>>>(dev_, tk); break;
+                case 1: mf::k_xinv_gemm<T, 0><<<nt, 256, kPairSmem, st>>>(dev_, tk); break;
+                default: mf::k_xinv_gemm<T, 1><<<nt, 256, kPairSmem, st>>>(dev_, tk); break;
                 }
             }
         }
@@ -810,7 +859,7 @@ public:
 
     // x = A^-1 b on the device (b and x may alias). The level sweeps run as one captured CUDA graph on the
     // solver's internal vector; only the permutations in and out are launched per call.
-    void solve(const double *d_b, double *d_x)
+    void solve(const double *d_b, double *d_x) override
     {
         if (!factored_) throw Failure(IFEA_BAD_STATE, "Factorize must be called first.");
         const MfSymbolic &S = sym_;
@@ -825,9 +874,9 @@ public:
             cuda_check(e, "cudaGraphInstantiate");
         }
         if (profile_) cuda_check(cudaEventRecord(ev_[2], st_), "cudaEventRecord");
-        mf::k_permute_in<<<g, 256, 0, st_>>>(n, d_perm_, d_b, d_y_);
+        mf::k_permute_in<T><<<g, 256, 0, st_>>>(n, d_perm_, d_b, d_y_);
         cuda_check(cudaGraphLaunch(solve_exec_, st_), "cudaGraphLaunch");
-        mf::k_permute_out<<<g, 256, 0, st_>>>(n, d_perm_, d_y_, d_x);
+        mf::k_permute_out<T><<<g, 256, 0, st_>>>(n, d_perm_, d_y_, d_x);
         n_solves_++;
         if (profile_) {
             cuda_check(cudaEventRecord(ev_[3], st_), "cudaEventRecord");
@@ -843,7 +892,7 @@ public:
         const MfSymbolic &S = sym_;
         for (int l = 0; l < S.nlevels; l++) {
             int q0 = small_start_[l], cnt = small_start_[l + 1] - q0;
-            if (cnt > 0) mf::k_forward<<<cnt, 512, small_smem_, st>>>(dev_, d_small_.p + q0, d_y_);
+            if (cnt > 0) mf::k_forward<T><<<cnt, 512, small_smem_, st>>>(dev_, d_small_.p + q0, d_y_);
             int b0 = big_start_[l], bc = big_start_[l + 1] - b0;
             if (bc > 0) {
                 int mnc = 1, mnr = 1;
@@ -851,24 +900,24 @@ public:
                     mnc = std::max(mnc, S.ncol[big_list_[q]]);
                     mnr = std::max(mnr, S.m[big_list_[q]] - S.ncol[big_list_[q]]);
                 }
-                mf::k_wide_fwd_acc<<<bc, 512, 0, st>>>(dev_, d_big_.p + b0, d_y_);
-                mf::k_wide_fwd_y<<<dim3((mnc + mf::RT - 1) / mf::RT, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
-                mf::k_wide_fwd_t<<<dim3((mnr + mf::RT - 1) / mf::RT, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
+                mf::k_wide_fwd_acc<T><<<bc, 512, 0, st>>>(dev_, d_big_.p + b0, d_y_);
+                mf::k_wide_fwd_y<T><<<dim3((mnc + mf::RT - 1) / mf::RT, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
+                mf::k_wide_fwd_t<T><<<dim3((mnr + mf::RT - 1) / mf::RT, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
             }
         }
         for (int l = S.nlevels - 1; l >= 0; l--) {
             int q0 = small_start_[l], cnt = small_start_[l + 1] - q0;
-            if (cnt > 0) mf::k_backward<<<cnt, 512, small_smem_, st>>>(dev_, d_small_.p + q0, d_y_, d_y_);
+            if (cnt > 0) mf::k_backward<T><<<cnt, 512, small_smem_, st>>>(dev_, d_small_.p + q0, d_y_, d_y_);
             int b0 = big_start_[l], bc = big_start_[l + 1] - b0;
             if (bc > 0) {
                 int mnc = S.ncol[big_list_[b0]];
-                mf::k_wide_bwd_z<<<dim3((mnc + 15) / 16, bc), 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_y_, d_z_);
-                mf::k_wide_bwd_x<<<dim3((mnc + 15) / 16, bc), 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
+                mf::k_wide_bwd_z<T><<<dim3((mnc + 15) / 16, bc), 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_y_, d_z_);
+                mf::k_wide_bwd_x<T><<<dim3((mnc + 15) / 16, bc), 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
             }
         }
     }
 
-    void check_finite(const double *d_x)
+    void check_finite(const double *d_x) override
     {
         int32_t zero = 0, f = 0;
         cuda_check(cudaMemcpyAsync(d_err_.p + 1, &zero, sizeof zero, cudaMemcpyHostToDevice, st_), "H2D");
@@ -893,9 +942,9 @@ private:
     cudaStream_t cap_ = nullptr;
     cudaGraphExec_t solve_exec_ = nullptr, factor_exec_ = nullptr;
     const double *factor_vals_ = nullptr;
-    static constexpr size_t kUpdateSmem = 2 * mf::UT * (mf::PW + 1) * sizeof(double);
-    static constexpr size_t kPairSmem = 2 * mf::PW * (mf::PW + 1) * sizeof(double);
-    static constexpr size_t kPanelSmem = kPairSmem + 32 * 33 * sizeof(double);
+    static constexpr size_t kUpdateSmem = 2 * mf::UT * (mf::PW + 1) * sizeof(T);
+    static constexpr size_t kPairSmem = 2 * mf::PW * (mf::PW + 1) * sizeof(T);
+    static constexpr size_t kPanelSmem = kPairSmem + 32 * 33 * sizeof(T);
     cudaStream_t st_;
     cusolverSpHandle_t hsp_ = nullptr;
     std::vector<int64_t> inv_off_, xinv_off_;
@@ -905,7 +954,7 @@ private:
     size_t small_smem_ = 8, wide_smem_ = 8;
     DBuf<int64_t> d_inv_off_, d_xinv_off_;
     DBuf<int32_t> d_small_, d_big_;
-    DBuf<double> d_Inv_, d_Xinv_, d_Abig_, d_y1_, d_z_;
+    DBuf<T> d_Inv_, d_Xinv_, d_Abig_, d_y1_, d_z_;
     cusparseMatDescr_t descr_ = nullptr;
     MfSymbolic sym_;
     bool analyzed_ = false, factored_ = false;
@@ -913,8 +962,10 @@ private:
     DBuf<int32_t> d_ncol_, d_m_, d_c0_, d_idxs_, d_idx_, d_rms_, d_rm_, d_uvs_, d_par_, d_perm_, d_asrc_, d_ext_, d_cs_,
         d_cl_, d_lvl_, d_err_;
     DBuf<int64_t> d_off_, d_adst_;
-    DBuf<double> d_F_, d_U_, d_y_;
-    mf::Dev dev_{};
+    DBuf<T> d_F_, d_U_, d_y_;
+    mf::Dev<T> dev_{};
 };
+
+using MfSolver = MfSolverT<double>;
 
 }  // namespace ifea

@@ -56,8 +56,11 @@ struct Forging3D {
     int last_cutbacks = 0, n_newton = 0, n_assemble = 0, lin_its = 0;
     double load = 0, reaction = 0, power = 0, last_dt = 0, rnorm = 0, beta_last = 0, max_diag = 0;
     // linear solver (SolveLinear :965-1019)
-    std::unique_ptr<MfSolver> lin;
+    std::unique_ptr<LinearSolver> lin;
     bool need_analyze = true, have_factor = false;
+    // single-precision factor refined by FP64 PCG (off: the reference's FP64 direct solve after a factorisation)
+    bool factor_fp32 = false;
+    int fp32_fallbacks = 0, refine_its = 0;
     int pcg_failures = 0, pcg_skip = 0;
     // mesh
     TetTopology topo;
@@ -116,6 +119,21 @@ struct Forging3D {
     }
 
     int grid(int n) const { return std::max(1, std::min((n + 255) / 256, 8 * 148)); }
+
+    // Switch the factorisation between double and single precision; the next solve analyses and factorises anew.
+    void use_precision(bool fp32)
+    {
+        if (fp32 == (lin->value_bytes() == 4)) return;
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        lin.reset();
+        if (fp32)
+            lin.reset(new MfSolverT<float>(st));
+        else
+            lin.reset(new MfSolverT<double>(st));
+        need_analyze = true;
+        have_factor = false;
+        pcg_skip = pcg_failures = 0;
+    }
 
     View3 view()
     {
@@ -403,9 +421,21 @@ struct Forging3D {
         }
         try {
             PhaseTimer pt(t_factor);
-            lin->factorize(d_val);
-            lin->solve(b, x);
-            lin->check_finite(x);
+            try {
+                lin->factorize(d_val);
+            } catch (Failure &f) {
+                // a pivot lost to single-precision rounding: continue in double precision for good
+                if (f.status != IFEA_NOT_SPD || lin->value_bytes() == 8) throw;
+                use_precision(false);
+                fp32_fallbacks++;
+                lin->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3);
+                need_analyze = false;
+                lin->factorize(d_val);
+            }
+            if (lin->value_bytes() == 8) {
+                lin->solve(b, x);
+                lin->check_finite(x);
+            }
         } catch (Failure &f) {
             have_factor = false;
             if (f.status == IFEA_NOT_SPD) throw;
@@ -413,6 +443,17 @@ struct Forging3D {
         }
         have_factor = true;
         n_fact++;
+        if (lin->value_bytes() != 8) {
+            // FP64 refinement of the single-precision factor's solution, to the tolerance of the reused-factor PCG
+            PhaseTimer pt(t_pcg);
+            int l0 = lin_its;
+            int its = pcg(b, x, 1e-7, P.pcg_budget);
+            refine_its += lin_its - l0;
+            if (its < 0) {
+                have_factor = false;
+                throw Failure(IFEA_DIVERGED, fmt("Refinement of the single-precision factor did not converge at step %d.", step_index));
+            }
+        }
         return 1;
     }
 
@@ -688,8 +729,9 @@ struct Forging3D {
         S("t_trigger", t_trigger) S("t_prepare", t_prepare) S("t_assemble", t_assemble) S("t_linesearch", t_linesearch)
         S("t_factor", t_factor) S("t_pcg", t_pcg) S("t_final", t_final) S("t_update", t_update) S("t_total", t_total)
         S("supernodes", lin->symbolic().nsuper) S("levels", lin->symbolic().nlevels)
-        S("front_pool_mb", lin->symbolic().pool * 8e-6) S("max_front", lin->symbolic().max_m) S("big_fronts", lin->big_fronts())
+        S("front_pool_mb", lin->symbolic().pool * lin->value_bytes() * 1e-6) S("max_front", lin->symbolic().max_m) S("big_fronts", lin->big_fronts())
         S("factor_gpu_ms", lin->factor_ms()) S("solve_gpu_ms", lin->solve_ms()) S("solves", lin->solves())
+        S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
 #undef S
         if (nm == "volume") return volume();
         if (nm == "min_quality") return min_quality(d_x);
@@ -702,6 +744,7 @@ struct Forging3D {
         else if (nm == "ds_cur") ds_cur = v;
         else if (nm == "warm") warm = (int)v;
         else if (nm == "profile_solves") lin->set_profile(v != 0);
+        else if (nm == "factor_fp32") use_precision(v != 0);
         else throw Failure(IFEA_INPUT_INVALID, "unknown scalar name '" + nm + "'");
     }
 };
