@@ -90,6 +90,10 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
         Xs[rr][c] = 0.0;
     }
     __syncthreads();
+    // the reciprocal of pivot k is formed in step k - 1 by the thread that finishes that diagonal entry, which
+    // keeps the division off the chain of barriers
+    if (tid == 0) sq[0] = T(1) / Ds[0][0];
+    __syncthreads();
     for (int k = 0; k < w; k++) {
         T d = Ds[k][k];
         if (!(d > 0)) {
@@ -97,8 +101,10 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
             return;  // every thread read the same pivot: a uniform exit
         }
         if (r > k) {
-            T a = Ds[r][k] / d;
+            T a = Ds[r][k] * sq[k];
+#pragma unroll 4
             for (int c = k + 1 + cg; c <= r; c += 4) Ds[r][c] -= a * Ds[c][k];
+            if (r == k + 1 && cg == 0) sq[r] = T(1) / Ds[r][r];
         }
         __syncthreads();
     }
@@ -196,13 +202,18 @@ static __global__ void __launch_bounds__(256) k_panel_trsm(Dev<T> D, const int32
 // doubling over 64-column blocks. The diagonal blocks are the panel inverses (k_xinv_diag). Then groups of 2^t
 // blocks merge their halves, top [g0, gm) and bottom [gm, g1): X21 = -X22 L21 X11, in two passes over the
 // 64 x 64 output tiles (bi in the bottom half, bj in the top half): T = L21 X11 (k_xinv_gemm<0>, stored transposed
-// in X's unused upper triangle), then X21 = -X22 T (k_xinv_gemm<1>). The tasks (front, bi, bj, gm) of one pass are
-// listed on the host; one CTA per task, each thread a 4 x 4 register block.
+// in X's unused upper triangle), then X21 = -X22 T (k_xinv_gemm<1>). The tasks of one pass are listed on the host;
+// one CTA per task, each thread a 4 x 4 register block. The passes run on a side stream, overlapping the
+// factorisation of the levels above (only the solves read X).
+struct XTask {
+    int s, bi, bj, kb0, kb1, slot, nslot, pad;  // front, output block, block range, partial slots
+};
+
 template <typename T>
-static __global__ void k_xinv_diag(Dev<T> D, const int4 *__restrict__ tasks)
+static __global__ void k_xinv_diag(Dev<T> D, const XTask *__restrict__ tasks)
 {
-    int4 tk = tasks[blockIdx.x];
-    int s = tk.x, bi = tk.y, nc = D.ncol[s], r0 = bi * PW, w = min(PW, nc - r0);
+    XTask tk = tasks[blockIdx.x];
+    int s = tk.s, bi = tk.bi, nc = D.ncol[s], r0 = bi * PW, w = min(PW, nc - r0);
     const T *Dinv = D.Inv + D.inv_off[s] + (int64_t)bi * PW * PW;
     T *X = D.Xinv + D.xinv_off[s];
     for (int t = threadIdx.x; t < PW * PW; t += blockDim.x) {
@@ -211,25 +222,37 @@ static __global__ void k_xinv_diag(Dev<T> D, const int4 *__restrict__ tasks)
     }
 }
 
+// k_xinv_gemm computes one 64 x 64 output tile over the block range [kb0, kb1): in place when slot < 0, else as a
+// partial tile into the workspace, summed by k_xinv_reduce in slot order (long ranges are split so that no CTA
+// runs much longer than the others).
+
 template <typename T, int PASS>
-static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev<T> D, const int4 *__restrict__ tasks)
+__device__ __forceinline__ void xinv_store(T *X, int nc, int r0, int c0, int r, int c, T v)
+{
+    if (PASS == 0)
+        X[(int64_t)(r0 + r) * nc + c0 + c] = v;  // T(r, c) stored at X(c0 + c, r0 + r)
+    else
+        X[(int64_t)(c0 + c) * nc + r0 + r] = -v;
+}
+
+template <typename T, int PASS>
+static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev<T> D, const XTask *__restrict__ tasks, T *__restrict__ W)
 {
     extern __shared__ __align__(16) unsigned char shm_raw[];
     T *shm = (T *)shm_raw;
     T (*A)[PW + 1] = (T (*)[PW + 1])shm;
     T (*B)[PW + 1] = (T (*)[PW + 1])(shm + PW * (PW + 1));
-    int4 tk = tasks[blockIdx.x];
-    int s = tk.x, bi = tk.y, bj = tk.z, gm = tk.w;
+    XTask tk = tasks[blockIdx.x];
+    int s = tk.s, bi = tk.bi, bj = tk.bj;
     int ms = D.m[s], nc = D.ncol[s];
     const T *F = D.F + D.front_off[s];
     T *X = D.Xinv + D.xinv_off[s];
     int r0 = bi * PW, c0 = bj * PW, wr = min(PW, nc - r0), wc = min(PW, nc - c0);
-    int kb0 = PASS == 0 ? bj : gm, kb1 = PASS == 0 ? gm : bi + 1;
     int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     T acc[4][4];
     for (int a = 0; a < 4; a++)
         for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
-    for (int bk = kb0; bk < kb1; bk++) {
+    for (int bk = tk.kb0; bk < tk.kb1; bk++) {
         int k0 = bk * PW, wk = min(PW, nc - k0);
         __syncthreads();
         for (int t = threadIdx.x; t < PW * PW; t += blockDim.x) {
@@ -253,15 +276,31 @@ static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev<T> D, const int4 *
                 for (int b = 0; b < 4; b++) acc[a][b] += a4[a] * b4[b];
         }
     }
+    T *Wt = tk.slot >= 0 ? W + (int64_t)tk.slot * PW * PW : nullptr;
     for (int a = 0; a < 4; a++)
         for (int b = 0; b < 4; b++) {
             int r = tx + 16 * a, c = ty + 16 * b;
-            if (r >= wr || c >= wc) continue;
-            if (PASS == 0)
-                X[(int64_t)(r0 + r) * nc + c0 + c] = acc[a][b];  // T(r, c) stored at X(c0 + c, r0 + r)
-            else
-                X[(int64_t)(c0 + c) * nc + r0 + r] = -acc[a][b];
+            if (Wt)
+                Wt[c * PW + r] = acc[a][b];
+            else if (r < wr && c < wc)
+                xinv_store<T, PASS>(X, nc, r0, c0, r, c, acc[a][b]);
         }
+}
+
+template <typename T, int PASS>
+static __global__ void k_xinv_reduce(Dev<T> D, const XTask *__restrict__ tasks, const T *__restrict__ W)
+{
+    XTask tk = tasks[blockIdx.x];
+    int nc = D.ncol[tk.s];
+    T *X = D.Xinv + D.xinv_off[tk.s];
+    int r0 = tk.bi * PW, c0 = tk.bj * PW, wr = min(PW, nc - r0), wc = min(PW, nc - c0);
+    for (int t = threadIdx.x; t < PW * PW; t += blockDim.x) {
+        int r = t % PW, c = t / PW;
+        if (r >= wr || c >= wc) continue;
+        T v = 0;
+        for (int q = 0; q < tk.nslot; q++) v += W[(int64_t)(tk.slot + q) * PW * PW + t];
+        xinv_store<T, PASS>(X, nc, r0, c0, r, c, v);
+    }
 }
 
 // ---------------------------------------------------------------- solves of wide supernodes (batched multi-CTA GEMVs)
@@ -604,6 +643,8 @@ public:
         cusparseSetMatIndexBase(descr_, CUSPARSE_INDEX_BASE_ZERO);
         d_err_.resize(2);
         cuda_check(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaEventCreateWithFlags(&join_ev_, cudaEventDisableTiming), "cudaEventCreate");
         for (auto &e : ev_) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
     }
     ~MfSolverT() override
@@ -611,6 +652,9 @@ public:
         drop_graphs();
         for (auto &e : ev_)
             if (e) cudaEventDestroy(e);
+        for (auto &e : fork_ev_) cudaEventDestroy(e);
+        if (join_ev_) cudaEventDestroy(join_ev_);
+        if (side_) cudaStreamDestroy(side_);
         if (cap_) cudaStreamDestroy(cap_);
         if (descr_) cusparseDestroyMatDescr(descr_);
         if (hsp_) cusolverSpDestroy(hsp_);
@@ -706,11 +750,12 @@ public:
         cuda_check(cudaFuncSetAttribute((const void *)mf::k_wide_bwd_z<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wide_smem_), "cudaFuncSetAttribute");
         cuda_check(cudaFuncSetAttribute((const void *)mf::k_wide_bwd_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wide_smem_), "cudaFuncSetAttribute");
         // inverse passes of the wide supernodes, per level: diagonal copies, then for groups of 2, 4, ... blocks
-        // the T pass and the X21 pass
-        std::vector<int4> tasks;
+        // the T pass and the X21 pass, each followed by its reduction when a block range was split
+        std::vector<mf::XTask> tasks;
         xinv_pass_start_.assign(S.nlevels + 1, 0);
         xinv_task_start_.assign(1, 0);
         xinv_pass_kind_.clear();
+        int64_t max_slots = 0;
         auto close_pass = [&](int kind) {
             if ((int)tasks.size() == xinv_task_start_.back()) return;
             xinv_pass_kind_.push_back(kind);
@@ -722,23 +767,44 @@ public:
             for (int q = big_start_[l]; q < big_start_[l + 1]; q++) {
                 int sn = big_list_[q], nb = (S.ncol[sn] + mf::PW - 1) / mf::PW;
                 nbmax = std::max(nbmax, nb);
-                for (int b = 0; b < nb; b++) tasks.push_back(make_int4(sn, b, b, 0));
+                for (int b = 0; b < nb; b++) tasks.push_back({sn, b, b, 0, 0, -1, 0, 0});
             }
             close_pass(0);
             for (int G = 2; G / 2 < nbmax; G *= 2)
-                for (int kind = 1; kind <= 2; kind++) {
+                for (int pass = 0; pass < 2; pass++) {
+                    std::vector<mf::XTask> reduce;
+                    int slots = 0;
                     for (int q = big_start_[l]; q < big_start_[l + 1]; q++) {
                         int sn = big_list_[q], nb = (S.ncol[sn] + mf::PW - 1) / mf::PW;
                         for (int g0 = 0; g0 + G / 2 < nb; g0 += G) {
                             int gm = g0 + G / 2, g1 = std::min(g0 + G, nb);
                             for (int bi = gm; bi < g1; bi++)
-                                for (int bj = g0; bj < gm; bj++) tasks.push_back(make_int4(sn, bi, bj, gm));
+                                for (int bj = g0; bj < gm; bj++) {
+                                    int kb0 = pass == 0 ? bj : gm, kb1 = pass == 0 ? gm : bi + 1;
+                                    if (kb1 - kb0 <= kXinvChunk) {
+                                        tasks.push_back({sn, bi, bj, kb0, kb1, -1, 0, 0});
+                                        continue;
+                                    }
+                                    int nch = (kb1 - kb0 + kXinvChunk - 1) / kXinvChunk;
+                                    for (int c = 0; c < nch; c++)
+                                        tasks.push_back({sn, bi, bj, kb0 + c * kXinvChunk,
+                                                         std::min(kb1, kb0 + (c + 1) * kXinvChunk), slots + c, 0, 0});
+                                    reduce.push_back({sn, bi, bj, 0, 0, slots, nch, 0});
+                                    slots += nch;
+                                }
                         }
                     }
-                    close_pass(kind);
+                    close_pass(1 + 2 * pass);
+                    tasks.insert(tasks.end(), reduce.begin(), reduce.end());
+                    close_pass(2 + 2 * pass);
+                    max_slots = std::max<int64_t>(max_slots, slots);
                 }
         }
         xinv_pass_start_[S.nlevels] = (int)xinv_pass_kind_.size();
+        for (auto &e : fork_ev_) cudaEventDestroy(e);
+        fork_ev_.assign(S.nlevels, nullptr);
+        for (auto &e : fork_ev_) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        d_xinv_w_.resize(std::max<int64_t>(max_slots * mf::PW * mf::PW, 1));
         d_xinv_tasks_.upload(tasks, st_);
         d_small_.upload(small_list_, st_);
         d_xinv_off_.upload(xinv_off_, st_);
@@ -810,6 +876,7 @@ public:
     void enqueue_factor(cudaStream_t st, const double *d_full_vals)
     {
         const MfSymbolic &S = sym_;
+        bool side_used = false;
         mf::k_init_err<<<1, 1, 0, st>>>(d_err_);
         for (int l = 0; l < S.nlevels; l++) {
             int64_t p0 = S.level_pool_start[l], p1 = S.level_pool_start[l + 1];
@@ -844,15 +911,26 @@ public:
                     mf::k_update<T><<<grid, 256, kUpdateSmem, st>>>(dev_, d_lvl_.p + q0, k0);
                 }
             }
+            if (xinv_pass_start_[l + 1] > xinv_pass_start_[l]) {
+                cuda_check(cudaEventRecord(fork_ev_[l], st), "cudaEventRecord");
+                cuda_check(cudaStreamWaitEvent(side_, fork_ev_[l], 0), "cudaStreamWaitEvent");
+                side_used = true;
+            }
             for (int pass = xinv_pass_start_[l]; pass < xinv_pass_start_[l + 1]; pass++) {
                 int t0 = xinv_task_start_[pass], nt = xinv_task_start_[pass + 1] - t0;
-                const int4 *tk = d_xinv_tasks_.p + t0;
+                const mf::XTask *tk = d_xinv_tasks_.p + t0;
                 switch (xinv_pass_kind_[pass]) {
-                case 0: mf::k_xinv_diag<T><<<nt, 256, 0, st>>>(dev_, tk); break;
-                case 1: mf::k_xinv_gemm<T, 0><<<nt, 256, kPairSmem, st>>>(dev_, tk); break;
-                default: mf::k_xinv_gemm<T, 1><<<nt, 256, kPairSmem, st>>>(dev_, tk); break;
+                case 0: mf::k_xinv_diag<T><<<nt, 256, 0, side_>>>(dev_, tk); break;
+                case 1: mf::k_xinv_gemm<T, 0><<<nt, 256, kPairSmem, side_>>>(dev_, tk, d_xinv_w_); break;
+                case 2: mf::k_xinv_reduce<T, 0><<<nt, 256, 0, side_>>>(dev_, tk, d_xinv_w_); break;
+                case 3: mf::k_xinv_gemm<T, 1><<<nt, 256, kPairSmem, side_>>>(dev_, tk, d_xinv_w_); break;
+                default: mf::k_xinv_reduce<T, 1><<<nt, 256, 0, side_>>>(dev_, tk, d_xinv_w_); break;
                 }
             }
+        }
+        if (side_used) {
+            cuda_check(cudaEventRecord(join_ev_, side_), "cudaEventRecord");
+            cuda_check(cudaStreamWaitEvent(st, join_ev_, 0), "cudaStreamWaitEvent");
         }
         cuda_check(cudaGetLastError(), "multifrontal factorisation launch");
     }
@@ -939,7 +1017,9 @@ private:
     double factor_ms_ = 0, solve_ms_ = 0;
     int64_t n_solves_ = 0;
     bool profile_ = false;
-    cudaStream_t cap_ = nullptr;
+    cudaStream_t cap_ = nullptr, side_ = nullptr;  // capture stream; side stream of the inverse passes
+    std::vector<cudaEvent_t> fork_ev_;
+    cudaEvent_t join_ev_ = nullptr;
     cudaGraphExec_t solve_exec_ = nullptr, factor_exec_ = nullptr;
     const double *factor_vals_ = nullptr;
     static constexpr size_t kUpdateSmem = 2 * mf::UT * (mf::PW + 1) * sizeof(T);
@@ -950,7 +1030,9 @@ private:
     std::vector<int64_t> inv_off_, xinv_off_;
     std::vector<int32_t> small_start_, small_list_, big_start_, big_list_;
     std::vector<int> xinv_pass_start_, xinv_task_start_, xinv_pass_kind_;
-    DBuf<int4> d_xinv_tasks_;
+    DBuf<mf::XTask> d_xinv_tasks_;
+    DBuf<T> d_xinv_w_;
+    static constexpr int kXinvChunk = 4;  // tile steps per CTA before a block range is split
     size_t small_smem_ = 8, wide_smem_ = 8;
     DBuf<int64_t> d_inv_off_, d_xinv_off_;
     DBuf<int32_t> d_small_, d_big_;
