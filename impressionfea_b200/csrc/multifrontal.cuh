@@ -7,7 +7,8 @@
 // eliminates the supernode's pivot columns in panels of 64: a one-CTA-per-front kernel factors the panel's
 // diagonal block in shared memory and solves the rows below it, and a tiled kernel subtracts the panel's
 // outer product from the trailing front. What remains in the trailing block is the update matrix the parent
-// reads; the pivot columns are the factor, so no copy is made. The solves walk the levels up (update vectors)
+// reads; the pivot columns are the factor, so no copy is made. Products are accumulated with explicit fused
+// multiply-adds (the library is built without contraction, which the element kernels' parity needs). The solves walk the levels up (update vectors)
 // and down (gathers from solved ancestors). Nothing uses atomics on values: results are bit-reproducible.
 #pragma once
 #include <cusolverSp.h>
@@ -62,10 +63,9 @@ static __global__ void k_extend(Dev<T> D, const int32_t *__restrict__ children, 
     }
 }
 
-// Panel k0 of every listed front: Cholesky of the diagonal block in shared memory and the block's inverse (kept
-// for the rows below and for the solves). The factorisation runs in the L D L^T form (the pivot column is scaled
-// only at the end), so each column costs one barrier; rows at or beyond the block width are padded with the
-// identity. The inverse is built by recursive doubling: the 8x8 diagonal blocks are inverted by forward
+// Panel k0 of every listed front: Cholesky of the diagonal block and the block's inverse (kept for the rows below
+// and for the solves). The factorisation runs in the L D L^T form on registers (the pivot column is scaled only at
+// the end), so each column costs one barrier; rows at or beyond the block width are padded with the identity. The inverse is built by recursive doubling: the 8x8 diagonal blocks are inverted by forward
 // substitution in registers, then pairs of blocks merge with X21 = -X22 L21 X11 at sizes 8, 16 and 32. The lowest
 // failing pivot column (new numbering) goes to err. Dynamic shared memory: two 64 x 65 blocks and a 32 x 33 one.
 template <typename T>
@@ -76,46 +76,76 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
     T (*Ds)[PW + 1] = (T (*)[PW + 1])shp;
     T (*Xs)[PW + 1] = (T (*)[PW + 1])(shp + PW * (PW + 1));
     T (*Ts)[33] = (T (*)[33])(shp + 2 * PW * (PW + 1));
-    __shared__ T sq[PW];
+    __shared__ T col[2][PW];  // column k of the active block (double-buffered by step parity)
+    __shared__ T piv[PW];     // reciprocal pivots during the sweep, then the square roots
+    __shared__ T rpiv[PW];    // reciprocal square roots of the pivots
     int s = fronts[blockIdx.x];
     int ms = D.m[s], w = min(PW, D.ncol[s] - k0);
     T *F = D.F + D.front_off[s];
     T *Inv = D.Inv + D.inv_off[s] + (int64_t)(k0 / PW) * PW * PW;
     int tid = threadIdx.x, r = tid & (PW - 1), cg = tid >> 6;
-    for (int t = tid; t < PW * PW; t += blockDim.x) {
-        int rr = t % PW, c = t / PW;
-        T v = rr == c ? 1.0 : 0.0;
-        if (rr < w && c < w && rr >= c) v = F[(int64_t)(k0 + c) * ms + k0 + rr];
-        Ds[rr][c] = v;
-        Xs[rr][c] = 0.0;
+    // thread (r, cg) keeps row r, columns c = cg + 4j, in registers; rows and columns at or beyond the block width
+    // are the identity
+    T R[PW / 4];
+#pragma unroll
+    for (int j = 0; j < PW / 4; j++) {
+        int c = cg + 4 * j;
+        T v = r == c ? T(1) : T(0);
+        if (r < w && c < w && r >= c) v = F[(int64_t)(k0 + c) * ms + k0 + r];
+        R[j] = v;
     }
+    if (cg == 0) {
+        col[0][r] = R[0];
+        if (r == 0) piv[0] = T(1) / R[0];
+    }
+    for (int t = tid; t < PW * (PW + 1); t += blockDim.x) (&Xs[0][0])[t] = T(0);
     __syncthreads();
-    // the reciprocal of pivot k is formed in step k - 1 by the thread that finishes that diagonal entry, which
-    // keeps the division off the chain of barriers
-    if (tid == 0) sq[0] = T(1) / Ds[0][0];
-    __syncthreads();
+    // column sweep: each step reads the published column k, updates the registers and publishes column k + 1
+    // (with its pivot's reciprocal, formed by the thread that finishes it); one barrier per column
     for (int k = 0; k < w; k++) {
-        T d = Ds[k][k];
+        const T *ck = col[k & 1];
+        T *cn = col[(k + 1) & 1];
+        T d = ck[k];
         if (!(d > 0)) {
             if (tid == 0) atomicMin(err, D.c0[s] + k0 + k);
             return;  // every thread read the same pivot: a uniform exit
         }
-        if (r > k) {
-            T a = Ds[r][k] * sq[k];
-#pragma unroll 4
-            for (int c = k + 1 + cg; c <= r; c += 4) Ds[r][c] -= a * Ds[c][k];
-            if (r == k + 1 && cg == 0) sq[r] = T(1) / Ds[r][r];
+        T a = ck[r] * piv[k];
+        int jn = (k + 1) >> 2;  // register slot of column k + 1 (owned by cg == (k + 1) & 3)
+        T nxt = T(0);
+#pragma unroll
+        for (int j = 0; j < PW / 4; j++) {
+            int c = cg + 4 * j;
+            T u = ck[c];
+            T v = fma(-a, u, R[j]);
+            R[j] = (c > k && c <= r) ? v : R[j];
+            nxt = j == jn ? R[j] : nxt;
+        }
+        if (cg == ((k + 1) & 3)) {
+            cn[r] = nxt;
+            if (r == k + 1) piv[r] = T(1) / nxt;
         }
         __syncthreads();
     }
-    if (tid < PW) sq[tid] = sqrt(Ds[tid][tid]);
-    __syncthreads();
-    for (int c = cg; c <= r; c += 4) Ds[r][c] = c == r ? sq[r] : Ds[r][c] / sq[c];
-    __syncthreads();
-    for (int t = tid; t < w * w; t += blockDim.x) {
-        int rr = t % w, c = t / w;
-        if (rr >= c) F[(int64_t)(k0 + c) * ms + k0 + rr] = Ds[rr][c];
+    {
+        T dg = T(0);
+#pragma unroll
+        for (int j = 0; j < PW / 4; j++) dg = cg + 4 * j == r ? R[j] : dg;
+        if (cg == (r & 3)) {
+            T q = sqrt(dg);
+            piv[r] = q;
+            rpiv[r] = T(1) / q;
+        }
     }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < PW / 4; j++) {
+        int c = cg + 4 * j;
+        T v = c == r ? piv[r] : c < r ? R[j] * rpiv[c] : T(0);
+        Ds[r][c] = v;
+        if (r < w && c < w && c <= r) F[(int64_t)(k0 + c) * ms + k0 + r] = v;
+    }
+    __syncthreads();
     // 8x8 diagonal blocks: thread (b, j) forward-substitutes column j of block b
     if (tid < PW) {
         int b8 = (tid >> 3) * 8, j = tid & 7;
@@ -124,7 +154,7 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
         for (int i = 0; i < 8; i++) {
             T v = i == j ? 1.0 : 0.0;
 #pragma unroll
-            for (int q = 0; q < i; q++) v -= Ds[b8 + i][b8 + q] * x[q];
+            for (int q = 0; q < i; q++) v = fma(-Ds[b8 + i][b8 + q], x[q], v);
             x[i] = v / Ds[b8 + i][b8 + i];
         }
 #pragma unroll
@@ -137,14 +167,14 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
         for (int t = tid; t < total; t += blockDim.x) {
             int p = t / per, e = t % per, i = e / h, j = e % h, b = p * 2 * h;
             T v = 0;
-            for (int q = j; q < h; q++) v += Ds[b + h + i][b + q] * Xs[b + q][b + j];
+            for (int q = j; q < h; q++) v = fma(Ds[b + h + i][b + q], Xs[b + q][b + j], v);
             Ts[p * h + i][j] = v;  // the pairs of one size fill 32 rows
         }
         __syncthreads();
         for (int t = tid; t < total; t += blockDim.x) {
             int p = t / per, e = t % per, i = e / h, j = e % h, b = p * 2 * h;
             T v = 0;
-            for (int q = 0; q <= i; q++) v += Xs[b + h + i][b + h + q] * Ts[p * h + q][j];
+            for (int q = 0; q <= i; q++) v = fma(Xs[b + h + i][b + h + q], Ts[p * h + q][j], v);
             Xs[b + h + i][b + j] = -v;
         }
         __syncthreads();
@@ -189,7 +219,7 @@ static __global__ void __launch_bounds__(256) k_panel_trsm(Dev<T> D, const int32
         for (int a = 0; a < 4; a++) f[a] = Ft[tx + 16 * a][l];
         for (int b = 0; b < 4; b++) d[b] = Di[ty + 16 * b][l];
         for (int a = 0; a < 4; a++)
-            for (int b = 0; b < 4; b++) acc[a][b] += f[a] * d[b];
+            for (int b = 0; b < 4; b++) acc[a][b] = fma(f[a], d[b], acc[a][b]);
     }
     for (int a = 0; a < 4; a++)
         for (int b = 0; b < 4; b++) {
@@ -273,7 +303,7 @@ static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev<T> D, const XTask 
             for (int a = 0; a < 4; a++) a4[a] = A[tx + 16 * a][k];
             for (int b = 0; b < 4; b++) b4[b] = B[k][ty + 16 * b];
             for (int a = 0; a < 4; a++)
-                for (int b = 0; b < 4; b++) acc[a][b] += a4[a] * b4[b];
+                for (int b = 0; b < 4; b++) acc[a][b] = fma(a4[a], b4[b], acc[a][b]);
         }
     }
     T *Wt = tk.slot >= 0 ? W + (int64_t)tk.slot * PW * PW : nullptr;
@@ -348,7 +378,7 @@ static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32
     if (r < nc) {
 #pragma unroll 8
         for (int c = sub; c < cend; c += 32)
-            if (c <= r) v += X[(int64_t)c * nc + r] * acc[c];
+            if (c <= r) v = fma(X[(int64_t)c * nc + r], acc[c], v);
     }
     part[sub][rr] = v;
     __syncthreads();
@@ -376,7 +406,7 @@ static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32
     T v = 0;
     if (i < nr) {
 #pragma unroll 8
-        for (int k = sub; k < nc; k += 32) v += F[(int64_t)k * ms + i] * y1[k];
+        for (int k = sub; k < nc; k += 32) v = fma(F[(int64_t)k * ms + i], y1[k], v);
     }
     part[sub][rr] = v;
     __syncthreads();
@@ -407,7 +437,7 @@ static __global__ void __launch_bounds__(512) k_wide_bwd_z(Dev<T> D, const int32
     int lane = threadIdx.x & 31;
     T v = 0;
 #pragma unroll 8
-    for (int i = lane; i < nr; i += 32) v += col[i] * xs[i];
+    for (int i = lane; i < nr; i += 32) v = fma(col[i], xs[i], v);
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) Z[D.idx_start[s] + k] = x[c0 + k] - v;
 }
@@ -432,7 +462,7 @@ static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev<T> D, const int32
     int lane = threadIdx.x & 31;
     T v = 0;
 #pragma unroll 8
-    for (int i = j + lane; i < nc; i += 32) v += col[i] * zs[i - jbase];
+    for (int i = j + lane; i < nc; i += 32) v = fma(col[i], zs[i - jbase], v);
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) x[c0 + j] = v;
 }
@@ -475,7 +505,7 @@ static __global__ void __launch_bounds__(256) k_update(Dev<T> D, const int32_t *
             for (int a = 0; a < 4; a++) ai[a] = Ai[tx + 16 * a][k];
             for (int b = 0; b < 4; b++) aj[b] = Aj[ty + 16 * b][k];
             for (int a = 0; a < 4; a++)
-                for (int b = 0; b < 4; b++) acc[a][b] += ai[a] * aj[b];
+                for (int b = 0; b < 4; b++) acc[a][b] = fma(ai[a], aj[b], acc[a][b]);
         }
         for (int a = 0; a < 4; a++)
             for (int b = 0; b < 4; b++) {
@@ -531,7 +561,7 @@ static __global__ void __launch_bounds__(512) k_forward(Dev<T> D, const int32_t 
         // y_blk = Linv acc_blk (warp per output row, coalesced over the inverse's columns? rows: I[c*PW + i])
         for (int i = warp; i < w; i += nw) {
             T v = 0;
-            for (int c = lane; c <= i; c += 32) v += I[(int64_t)c * PW + i] * acc[kb + c];
+            for (int c = lane; c <= i; c += 32) v = fma(I[(int64_t)c * PW + i], acc[kb + c], v);
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) yb[i] = v;
         }
@@ -540,7 +570,7 @@ static __global__ void __launch_bounds__(512) k_forward(Dev<T> D, const int32_t 
         // rows below the block
         for (int r = kb + w + tid; r < ms; r += nt) {
             T v = acc[r];
-            for (int k = 0; k < w; k++) v -= F[(int64_t)(kb + k) * ms + r] * yb[k];
+            for (int k = 0; k < w; k++) v = fma(-F[(int64_t)(kb + k) * ms + r], yb[k], v);
             acc[r] = v;
         }
         __syncthreads();
@@ -570,7 +600,7 @@ static __global__ void __launch_bounds__(512) k_backward(Dev<T> D, const int32_t
     for (int k = warp; k < nc; k += nw) {
         const T *col = F + (int64_t)k * ms + nc;
         T v = 0;
-        for (int i = lane; i < nr; i += 32) v += col[i] * xs[i];
+        for (int i = lane; i < nr; i += 32) v = fma(col[i], xs[i], v);
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
         if (lane == 0) acc[k] -= v;
     }
@@ -581,7 +611,7 @@ static __global__ void __launch_bounds__(512) k_backward(Dev<T> D, const int32_t
         for (int j = kb + warp; j < ke; j += nw) {
             const T *col = F + (int64_t)j * ms;
             T v = 0;
-            for (int k = ke + lane; k < nc; k += 32) v += col[k] * acc[k];
+            for (int k = ke + lane; k < nc; k += 32) v = fma(col[k], acc[k], v);
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) acc[j] -= v;
         }
@@ -590,7 +620,7 @@ static __global__ void __launch_bounds__(512) k_backward(Dev<T> D, const int32_t
         const T *I = Inv + (int64_t)bi * PW * PW;
         for (int j = warp; j < w; j += nw) {
             T v = 0;
-            for (int i = j + lane; i < w; i += 32) v += I[(int64_t)j * PW + i] * acc[kb + i];
+            for (int i = j + lane; i < w; i += 32) v = fma(I[(int64_t)j * PW + i], acc[kb + i], v);
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) xb[j] = v;
         }
