@@ -1,4 +1,4 @@
-"""Benchmark: stroke increments per second of the 3D upsetting drop-in (plain FP64) on B200.
+"""Benchmark: stroke increments per second of the 3D upsetting drop-in on B200, FP32-factor form vs plain FP64.
 
 Workload (one "step" = one forging increment, Forging3DSolver.Step): quarter model of a cylindrical billet
 d = 30 mm, h = 45 mm, ~30k linear tets (seeded Delaunay fill, node jitter +-10 % of h), flat dies as two-triangle
@@ -6,7 +6,10 @@ height fields, C = 150 MPa, eps0 = 0.01, n = 0.1, m = 0.12, friction m_f = 0.4, 
 increments (ds = 0.225 mm), reference defaults otherwise (ram 50 mm/s, tolerance 1e-3). Synthetic data.
 
 Arms:
-  default            the CUDA path (libifea_gpu.so) — one JSON line, device-timed with CUDA events;
+  default            the CUDA path (libifea_gpu.so) — one JSON line, device-timed with CUDA events. `value` is the
+                     single-precision-factor form (FP32 multifrontal Cholesky, every solve refined by FP64 PCG to
+                     1e-7); `plain_fp64` is the reference's arithmetic (FP64 factor, direct solve) on the same
+                     increments, and `error_vs_plain_fp64` compares the two increment by increment;
   --impl reference   the reference algorithm on the host cores (the C# reference cannot run here; its CPU
                      restatement under oracle/ is timed instead, OpenMP element phase on all host threads).
 
@@ -45,7 +48,7 @@ def workload():
 
 
 def config_dict(cfg, mesh, extra=None):
-    d = {"workload": "3D upsetting drop-in, plain FP64 (quarter cylinder d30 x h45, flat dies, 40% in 80 steps)",
+    d = {"workload": "3D upsetting drop-in (quarter cylinder d30 x h45, flat dies, 40% in 80 steps)",
          "tets": int(mesh.ne), "nodes": int(mesh.nn), "dof": int(3 * mesh.nn), "h_mm": cfg.h, "ds_mm": cfg.ds,
          "friction": cfg.friction, "tolerance": cfg.tol, "global_batch": 1, "parallelism": "replicas"}
     if extra:
@@ -147,6 +150,56 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def _timed_steps(s, stream, flush, k, snap=None):
+    """k increments of solver s, each bracketed by CUDA events on the solver's stream, L2 flushed in between."""
+    import torch
+
+    durs, infos, snaps = [], [], []
+    for _ in range(k):
+        if s.IsFinished:
+            break
+        flush.zero_()  # L2 flush between timed increments (outside the timed pair)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        infos.append(s.step())
+        b.record(stream)
+        b.synchronize()
+        durs.append(a.elapsed_time(b))
+        if snap:
+            snaps.append({nm: s.array(nm).copy() for nm in snap})
+    return durs, infos, snaps
+
+
+def _count_launches(cfg, mesh, dies, stream, warmup, k, fp32):
+    """Kernels of this library launched during k increments (after the same warm-up), counted by the CUDA
+    profiler interface on a re-run of the timed increments."""
+    import torch
+
+    from impressionfea_b200.forging3d import Forging3DSolver
+
+    try:
+        s = Forging3DSolver(cfg, mesh, dies)
+        s.set_stream(stream.cuda_stream)
+        if fp32:
+            s.set_scalar("factor_fp32", 1)
+        for _ in range(warmup):
+            s.step()
+        torch.cuda.synchronize()
+        acts = [torch.profiler.ProfilerActivity.CUDA]
+        with torch.profiler.profile(activities=acts) as prof:
+            for _ in range(k):
+                s.step()
+            torch.cuda.synchronize()
+        s.close()
+        n = 0
+        for e in prof.events():
+            if e.device_type == torch.autograd.DeviceType.CUDA and "k_" in e.name and "at::" not in e.name:
+                n += 1
+        return n
+    except Exception:
+        return None
+
+
 def run_gpu(args, rank, world):
     import torch
 
@@ -160,26 +213,28 @@ def run_gpu(args, rank, world):
     cfg, mesh, dies = workload()
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    snap = ("vg", "eps")
+
+    # plain FP64 form (the reference's arithmetic: FP64 factorisation, direct solve after each factorisation)
+    s64 = Forging3DSolver(cfg, mesh, dies)
+    s64.set_stream(stream.cuda_stream)
+    for _ in range(args.warmup):
+        s64.step()
+    torch.cuda.synchronize()
+    durs64, infos64, snaps64 = _timed_steps(s64, stream, flush, args.steps, snap)
+
+    # FP32 factorisation refined by FP64 PCG: the timed form
     s = Forging3DSolver(cfg, mesh, dies)
     s.set_stream(stream.cuda_stream)
+    s.set_scalar("factor_fp32", 1)
     for _ in range(args.warmup):
         s.step()
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    durs, infos = [], []
     with ClockSampler(dev) as clk:
-        for _ in range(args.steps):
-            if s.IsFinished:
-                break
-            flush.zero_()  # L2 flush between timed increments (outside the timed pair)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            infos.append(s.step())
-            b.record(stream)
-            b.synchronize()
-            durs.append(a.elapsed_time(b))
+        durs, infos, snaps = _timed_steps(s, stream, flush, args.steps, snap)
     torch.cuda.synchronize()
     k = len(durs)
     total_ms = float(sum(durs))
@@ -189,8 +244,42 @@ def run_gpu(args, rank, world):
         total_ms = float(t.item())
         torch.distributed.barrier()
     value = world * k / (total_ms / 1000.0)
+    ms64 = float(sum(durs64)) / max(len(durs64), 1)
 
-    # roofline of the dominant kernel of this library: the matrix assembly (element + column kernels)
+    # error of the timed form against the plain FP64 form, increment by increment
+    kk = min(len(infos), len(infos64))
+    load_err = max((abs(infos[i]["load"] / infos64[i]["load"] - 1) for i in range(kk)), default=None)
+    vel_err = max((float(np.linalg.norm(snaps[i]["vg"] - snaps64[i]["vg"]) / np.linalg.norm(snaps64[i]["vg"]))
+                   for i in range(kk)), default=None)
+    eps_err = max((float(np.linalg.norm(snaps[i]["eps"] - snaps64[i]["eps"]) / max(np.linalg.norm(snaps64[i]["eps"]), 1e-300))
+                   for i in range(kk)), default=None)
+
+    # roofline: the factor's triangular-solve sweep (forward + backward over every front, one captured graph per
+    # solve), HBM-bound; algorithmic bytes = the factor read once per sweep direction (a wide front's pivot-block
+    # inverse has as many entries as the triangle it replaces) plus the permuted vectors in and out
+    s.set_scalar("profile_solves", 1)  # events around every solve (a host wait each): after the timed region
+    solves0, solve_ms0 = s.scalar("solves"), s.scalar("solve_gpu_ms")
+    for _ in range(2):
+        s.step()
+    n_solves = s.scalar("solves") - solves0
+    solve_ms = (s.scalar("solve_gpu_ms") - solve_ms0) / max(n_solves, 1)
+    s.set_scalar("profile_solves", 0)
+    vb = 4
+    lnnz = s.scalar("factor_nnz")
+    ndof = 3 * mesh.nn
+    sbytes = 2 * lnnz * vb + ndof * (8 + 8 + 4 * vb)
+    peak, peak_kind = measured_peak()
+    achieved = sbytes / (solve_ms / 1000.0) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "solve_traffic.json")
+    if os.path.exists(tp):
+        try:
+            with open(tp) as f:
+                traffic = json.load(f).get("bytes_per_solve")
+        except Exception:
+            traffic = None
+
+    # assembly (element + column kernels), the per-iteration HBM pass the element path is measured by
     nnz = int(s.scalar("nnz"))
     s.prepare_step()
     for _ in range(3):
@@ -206,22 +295,14 @@ def run_gpu(args, rank, world):
         asm.append(a.elapsed_time(b))
     asm_ms = float(np.median(asm))
     abytes = assembly_algorithmic_bytes(mesh.ne, mesh.nn, nnz)
-    peak, peak_kind = measured_peak()
-    achieved = abytes / (asm_ms / 1000.0) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "assembly_traffic.json")
-    if os.path.exists(tp):
-        try:
-            with open(tp) as f:
-                traffic = json.load(f).get("bytes_per_assembly")
-        except Exception:
-            traffic = None
+    a_achieved = abytes / (asm_ms / 1000.0) / 1e9
 
     # end to end through the public API with host buffers: mesh/die upload, K increments, snapshot read-back
     e2e_steps = min(args.steps, 10)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s2 = Forging3DSolver(cfg, mesh, dies)
+    s2.set_scalar("factor_fp32", 1)
     d2h = 0
     for _ in range(e2e_steps):
         s2.step()
@@ -231,23 +312,30 @@ def run_gpu(args, rank, world):
     s2.close()
     h2d = mesh.x.nbytes + mesh.tets.nbytes + mesh.on_x0.nbytes + mesh.on_y0.nbytes + sum(d.h.nbytes for d in dies)
 
-    gpu_launches = None
+    gpu_launches = _count_launches(cfg, mesh, dies, stream, args.warmup, k, True) if rank == 0 else None
     if rank == 0:
         clocks = clk.summary()
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": k, "warmup": args.warmup,
                 "ms_per_step": total_ms / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic",
-                "config": config_dict(cfg, mesh, {"l2": "flushed (256 MiB write) between timed increments",
-                                                  "newton_iterations": int(sum(i["iterations"] for i in infos)),
-                                                  "factorisations": int(infos[-1]["n_factor"]) if infos else 0,
-                                                  "pcg_solves": int(infos[-1]["n_pcg"]) if infos else 0,
-                                                  "load_last_N": infos[-1]["load"] if infos else None,
-                                                  "factor": {k: s.scalar(k) for k in ("supernodes", "levels", "front_pool_mb",
-                                                                                        "max_front", "factor_nnz")}}),
-                "roofline": {"kernel": "assembly (k_element<MATRIX> + k_columns<MATRIX,BC>)", "bound": "hbm",
-                             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                             "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes": abytes,
-                             "ms_per_launch": asm_ms},
+                "dtype": "f64 (factorisation f32, refined in f64)", "data": "synthetic",
+                "config": config_dict(cfg, mesh, {
+                    "form": "FP32 multifrontal factor + FP64 PCG refinement (no learned warm start)",
+                    "l2": "flushed (256 MiB write) between timed increments",
+                    "newton_iterations": int(sum(i["iterations"] for i in infos)),
+                    "factorisations": int(infos[-1]["n_factor"] - infos[0]["n_factor"]) + 1 if infos else 0,
+                    "factor": {q: s.scalar(q) for q in ("supernodes", "levels", "front_pool_mb", "max_front",
+                                                        "factor_nnz")}}),
+                "plain_fp64": {"value": 1000.0 / ms64, "unit": UNIT, "ms_per_step": ms64, "steps": len(durs64),
+                               "speedup_of_value": value / world / (1000.0 / ms64)},
+                "error_vs_plain_fp64": {"load_rel_max": load_err, "velocity_rel_l2_max": vel_err,
+                                        "strain_rel_l2_max": eps_err, "increments": kk},
+                "roofline": {"kernel": "multifrontal triangular-solve sweep (forward + backward, one graph per solve)",
+                             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                             "algorithmic_bytes": sbytes, "ms_per_launch": solve_ms, "launches": int(n_solves)},
+                "roofline_assembly": {"kernel": "assembly (k_element<MATRIX> + k_columns<MATRIX,BC>)", "bound": "hbm",
+                                      "achieved": a_achieved, "peak": peak, "unit": "GB/s", "frac": a_achieved / peak,
+                                      "peak_kind": peak_kind, "algorithmic_bytes": abytes, "ms_per_launch": asm_ms},
                 "e2e": {"value": e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
                         "d2h_bytes_per_step": d2h / e2e_steps},
                 "gpu_launches": gpu_launches, "clocks": clocks}
@@ -255,6 +343,7 @@ def run_gpu(args, rank, world):
             line["cpu_baseline"] = cpu_baseline_sample(budget_s=args.cpu_budget)
         print(json.dumps(line))
     s.close()
+    s64.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

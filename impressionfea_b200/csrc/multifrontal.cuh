@@ -338,9 +338,8 @@ static __global__ void k_xinv_reduce(Dev<T> D, const XTask *__restrict__ tasks, 
 
 // acc = [b(cols); 0] - children's update vectors (in child order).
 template <typename T>
-static __global__ void k_wide_fwd_acc(Dev<T> D, const int32_t *__restrict__ fronts, const T *y)
+__device__ __forceinline__ void dev_wide_acc(Dev<T> D, int s, const T *y)
 {
-    int s = fronts[blockIdx.x];
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s];
     T *acc = D.Abig + D.idx_start[s];
     for (int k = threadIdx.x; k < ms; k += blockDim.x) acc[k] = k < nc ? y[c0 + k] : 0.0;
@@ -420,13 +419,12 @@ static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32
 
 // z = y1 - L21^T x2, one warp per pivot column; x2 is gathered into shared memory once per CTA.
 template <typename T>
-static __global__ void __launch_bounds__(512) k_wide_bwd_z(Dev<T> D, const int32_t *__restrict__ fronts, const T *x, T *Z)
+__device__ __forceinline__ void dev_wide_bwd_z(Dev<T> D, int s, int tile, const T *x, T *Z)
 {
     extern __shared__ __align__(16) unsigned char xs_raw[];
     T *xs = (T *)xs_raw;
-    int s = fronts[blockIdx.y];
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s], nr = ms - nc;
-    int kbase = blockIdx.x * (blockDim.x >> 5);
+    int kbase = tile * (blockDim.x >> 5);
     if (kbase >= nc) return;
     const int32_t *ix = D.idx + D.idx_start[s] + nc;
     for (int i = threadIdx.x; i < nr; i += blockDim.x) xs[i] = x[ix[i]];
@@ -535,12 +533,11 @@ static __global__ void k_permute_out(int n, const int32_t *perm, const T *y, dou
 // Forward elimination of the fronts of one level: y(cols) and the update vector for the parent. Each 64-pivot
 // block is applied through its stored inverse (one block GEMV) instead of 64 dependent steps.
 template <typename T>
-static __global__ void __launch_bounds__(512) k_forward(Dev<T> D, const int32_t *__restrict__ fronts, T *y)
+__device__ __forceinline__ void dev_forward(Dev<T> D, int s, T *y)
 {
     extern __shared__ __align__(16) unsigned char acc_raw[];
     T *acc = (T *)acc_raw;
     __shared__ T yb[PW];
-    int s = fronts[blockIdx.x];
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s];
     const T *F = D.F + D.front_off[s];
     const T *Inv = D.Inv + D.inv_off[s];
@@ -582,12 +579,11 @@ static __global__ void __launch_bounds__(512) k_forward(Dev<T> D, const int32_t 
 
 // Back substitution of the fronts of one level: x(cols) from y(cols) and the solved ancestors' x.
 template <typename T>
-static __global__ void __launch_bounds__(512) k_backward(Dev<T> D, const int32_t *__restrict__ fronts, const T *y, T *x)
+__device__ __forceinline__ void dev_backward(Dev<T> D, int s, const T *y, T *x)
 {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     T *sm = (T *)sm_raw;
     __shared__ T xb[PW];
-    int s = fronts[blockIdx.x];
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s], nr = ms - nc;
     const T *F = D.F + D.front_off[s];
     const T *Inv = D.Inv + D.inv_off[s];
@@ -629,6 +625,31 @@ static __global__ void __launch_bounds__(512) k_backward(Dev<T> D, const int32_t
         __syncthreads();
     }
     for (int k = tid; k < nc; k += nt) x[c0 + k] = acc[k];
+}
+
+// One launch per level and sweep direction covers both kinds of front: the small fronts (one CTA each, whole
+// elimination) and the first phase of the wide ones (the assembled right-hand side going up, z = y1 - L21^T x2
+// coming down).
+template <typename T>
+static __global__ void __launch_bounds__(512) k_fwd_level(Dev<T> D, const int32_t *__restrict__ small, int nsmall,
+                                                          const int32_t *__restrict__ big, T *y)
+{
+    if ((int)blockIdx.x < nsmall)
+        dev_forward(D, small[blockIdx.x], y);
+    else
+        dev_wide_acc(D, big[blockIdx.x - nsmall], y);
+}
+
+template <typename T>
+static __global__ void __launch_bounds__(512) k_bwd_level(Dev<T> D, const int32_t *__restrict__ small, int nsmall,
+                                                          const int32_t *__restrict__ big, int ntz, T *x, T *Z)
+{
+    if ((int)blockIdx.x < nsmall) {
+        dev_backward(D, small[blockIdx.x], x, x);
+    } else {
+        int t = blockIdx.x - nsmall;
+        dev_wide_bwd_z(D, big[t / ntz], t % ntz, x, Z);
+    }
 }
 
 static __global__ void k_finite(int n, const double *x, int *flag)
@@ -777,7 +798,6 @@ public:
         wide_smem_ = 8;
         for (int sn : big_list_) wide_smem_ = std::max(wide_smem_, (size_t)std::max(S.ncol[sn], S.m[sn] - S.ncol[sn]) * sizeof(T));
         if (wide_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the wide solve kernels' shared-memory window");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_wide_bwd_z<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wide_smem_), "cudaFuncSetAttribute");
         cuda_check(cudaFuncSetAttribute((const void *)mf::k_wide_bwd_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wide_smem_), "cudaFuncSetAttribute");
         // inverse passes of the wide supernodes, per level: diagonal copies, then for groups of 2, 4, ... blocks
         // the T pass and the X21 pass, each followed by its reduction when a block range was split
@@ -862,8 +882,9 @@ public:
         cuda_check(cudaFuncSetAttribute((const void *)mf::k_xinv_gemm<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kPairSmem), "cudaFuncSetAttribute");
         if (small_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the solve kernels' shared-memory window");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_forward<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_smem_), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_backward<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_smem_), "cudaFuncSetAttribute");
+        level_smem_ = std::max(small_smem_, wide_smem_);
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_fwd_level<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_smem_), "cudaFuncSetAttribute");
+        cuda_check(cudaFuncSetAttribute((const void *)mf::k_bwd_level<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)level_smem_), "cudaFuncSetAttribute");
         cuda_check(cudaStreamSynchronize(st_), "cudaStreamSynchronize");
         analyzed_ = true;
     }
@@ -1000,28 +1021,28 @@ public:
         const MfSymbolic &S = sym_;
         for (int l = 0; l < S.nlevels; l++) {
             int q0 = small_start_[l], cnt = small_start_[l + 1] - q0;
-            if (cnt > 0) mf::k_forward<T><<<cnt, 512, small_smem_, st>>>(dev_, d_small_.p + q0, d_y_);
             int b0 = big_start_[l], bc = big_start_[l + 1] - b0;
+            if (cnt + bc > 0)
+                mf::k_fwd_level<T><<<cnt + bc, 512, small_smem_, st>>>(dev_, d_small_.p + q0, cnt, d_big_.p + b0, d_y_);
             if (bc > 0) {
                 int mnc = 1, mnr = 1;
                 for (int q = b0; q < b0 + bc; q++) {
                     mnc = std::max(mnc, S.ncol[big_list_[q]]);
                     mnr = std::max(mnr, S.m[big_list_[q]] - S.ncol[big_list_[q]]);
                 }
-                mf::k_wide_fwd_acc<T><<<bc, 512, 0, st>>>(dev_, d_big_.p + b0, d_y_);
                 mf::k_wide_fwd_y<T><<<dim3((mnc + mf::RT - 1) / mf::RT, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
                 mf::k_wide_fwd_t<T><<<dim3((mnr + mf::RT - 1) / mf::RT, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
             }
         }
         for (int l = S.nlevels - 1; l >= 0; l--) {
             int q0 = small_start_[l], cnt = small_start_[l + 1] - q0;
-            if (cnt > 0) mf::k_backward<T><<<cnt, 512, small_smem_, st>>>(dev_, d_small_.p + q0, d_y_, d_y_);
             int b0 = big_start_[l], bc = big_start_[l + 1] - b0;
-            if (bc > 0) {
-                int mnc = S.ncol[big_list_[b0]];
-                mf::k_wide_bwd_z<T><<<dim3((mnc + 15) / 16, bc), 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_y_, d_z_);
-                mf::k_wide_bwd_x<T><<<dim3((mnc + 15) / 16, bc), 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
-            }
+            int ntz = bc > 0 ? (S.ncol[big_list_[b0]] + 15) / 16 : 1;
+            if (cnt + bc > 0)
+                mf::k_bwd_level<T><<<cnt + bc * ntz, 512, level_smem_, st>>>(dev_, d_small_.p + q0, cnt, d_big_.p + b0, ntz,
+                                                                            d_y_, d_z_);
+            if (bc > 0)
+                mf::k_wide_bwd_x<T><<<dim3(ntz, bc), 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
         }
     }
 
@@ -1063,7 +1084,7 @@ private:
     DBuf<mf::XTask> d_xinv_tasks_;
     DBuf<T> d_xinv_w_;
     static constexpr int kXinvChunk = 4;  // tile steps per CTA before a block range is split
-    size_t small_smem_ = 8, wide_smem_ = 8;
+    size_t small_smem_ = 8, wide_smem_ = 8, level_smem_ = 8;
     DBuf<int64_t> d_inv_off_, d_xinv_off_;
     DBuf<int32_t> d_small_, d_big_;
     DBuf<T> d_Inv_, d_Xinv_, d_Abig_, d_y1_, d_z_;

@@ -61,7 +61,10 @@ struct Forging3D {
     // single-precision factor refined by FP64 PCG (off: the reference's FP64 direct solve after a factorisation)
     bool factor_fp32 = false;
     int fp32_fallbacks = 0, refine_its = 0;
-    int pcg_failures = 0, pcg_skip = 0;
+    // give up a reused-factor PCG as soon as its contraction rate shows it cannot meet the budget (on with the
+    // single-precision factor; off in the reference's FP64 form, whose iteration counts it must reproduce)
+    bool pcg_early_abort = false;
+    int pcg_failures = 0, pcg_skip = 0, pcg_failures_total = 0;
     // mesh
     TetTopology topo;
     int have_dies = 0;
@@ -380,8 +383,14 @@ struct Forging3D {
         k_dot2<<<kReduceBlocks, 256, 0, st>>>(V, d_pr, d_pz, S_RZ, d_pr, S_RR);
         finalize({S_RZ, S_RR});
         double rr = read_scalars()[S_RR];
+        double r0 = sqrt(rr);
         for (int it = 0; it < max_it; it++) {
             if (sqrt(rr) <= tol * bnorm) return it;
+            if (pcg_early_abort && it >= 3) {
+                // the observed contraction cannot reach the tolerance within the budget: refactorise now
+                double rate = pow(sqrt(rr) / r0, 1.0 / it);
+                if (!(rate < 1) || it + log(tol * bnorm / sqrt(rr)) / log(rate) > max_it) return -1;
+            }
             k_spmv<<<sp_grid, 256, 0, st>>>(V, d_pp, d_pq);
             k_dot2<<<kReduceBlocks, 256, 0, st>>>(V, d_pp, d_pq, S_PQ, nullptr, 0);
             finalize({S_PQ});
@@ -413,6 +422,7 @@ struct Forging3D {
                 n_pcg++;
                 return 0;
             }
+            pcg_failures_total++;
             if (++pcg_failures >= 2) pcg_skip = std::min(64, 1 << (pcg_failures - 1));
         }
         if (need_analyze) {
@@ -732,6 +742,7 @@ struct Forging3D {
         S("front_pool_mb", lin->symbolic().pool * lin->value_bytes() * 1e-6) S("max_front", lin->symbolic().max_m) S("big_fronts", lin->big_fronts())
         S("factor_gpu_ms", lin->factor_ms()) S("solve_gpu_ms", lin->solve_ms()) S("solves", lin->solves())
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
+        S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total)
 #undef S
         if (nm == "volume") return volume();
         if (nm == "min_quality") return min_quality(d_x);
@@ -744,7 +755,10 @@ struct Forging3D {
         else if (nm == "ds_cur") ds_cur = v;
         else if (nm == "warm") warm = (int)v;
         else if (nm == "profile_solves") lin->set_profile(v != 0);
-        else if (nm == "factor_fp32") use_precision(v != 0);
+        else if (nm == "factor_fp32") {
+            use_precision(v != 0);
+            pcg_early_abort = v != 0;
+        } else if (nm == "pcg_early_abort") pcg_early_abort = v != 0;
         else throw Failure(IFEA_INPUT_INVALID, "unknown scalar name '" + nm + "'");
     }
 };
