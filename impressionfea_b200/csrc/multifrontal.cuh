@@ -63,11 +63,37 @@ static __global__ void k_extend(Dev<T> D, const int32_t *__restrict__ children, 
     }
 }
 
+// Recursive-doubling merge of the panel inverse at block size H: for every pair of H x H diagonal blocks,
+// X21 = -X22 (L21 X11). The upper triangles of X11 and X22 are zero, so the dot products run over whole blocks.
+template <typename T, int H>
+__device__ __forceinline__ void panel_merge(T (*Ds)[PW + 1], T (*Xs)[PW + 1], T (*Ts)[33], int tid)
+{
+    constexpr int PER = H * H, TOTAL = (PW / (2 * H)) * PER;
+    for (int t = tid; t < TOTAL; t += 256) {
+        int p = t / PER, e = t % PER, i = e / H, j = e % H, b = p * 2 * H;
+        T v = 0;
+#pragma unroll
+        for (int q = 0; q < H; q++) v = fma(Ds[b + H + i][b + q], Xs[b + q][b + j], v);
+        Ts[p * H + i][j] = v;  // the pairs of one size fill 32 rows
+    }
+    __syncthreads();
+    for (int t = tid; t < TOTAL; t += 256) {
+        int p = t / PER, e = t % PER, i = e / H, j = e % H, b = p * 2 * H;
+        T v = 0;
+#pragma unroll
+        for (int q = 0; q < H; q++) v = fma(Xs[b + H + i][b + H + q], Ts[p * H + q][j], v);
+        Xs[b + H + i][b + j] = -v;
+    }
+    __syncthreads();
+}
+
 // Panel k0 of every listed front: Cholesky of the diagonal block and the block's inverse (kept for the rows below
-// and for the solves). The factorisation runs in the L D L^T form on registers (the pivot column is scaled only at
-// the end), so each column costs one barrier; rows at or beyond the block width are padded with the identity. The inverse is built by recursive doubling: the 8x8 diagonal blocks are inverted by forward
-// substitution in registers, then pairs of blocks merge with X21 = -X22 L21 X11 at sizes 8, 16 and 32. The lowest
-// failing pivot column (new numbering) goes to err. Dynamic shared memory: two 64 x 65 blocks and a 32 x 33 one.
+// and for the solves). Blocked L D L^T in shared memory: warp 0 factors eight columns at a time over all rows
+// below them (warp shuffles, no block barrier), then the whole CTA applies the eight columns to the trailing
+// block; the pivot columns are scaled to Cholesky form at the end. Rows and columns at or beyond the block width
+// are the identity. The inverse is built by recursive doubling: the 8x8 diagonal blocks by forward substitution in
+// registers, then merges at sizes 8, 16 and 32. The lowest failing pivot column (new numbering) goes to err.
+// Dynamic shared memory: two 64 x 65 blocks and a 32 x 33 one.
 template <typename T>
 static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *__restrict__ fronts, int k0, int *err)
 {
@@ -76,83 +102,96 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
     T (*Ds)[PW + 1] = (T (*)[PW + 1])shp;
     T (*Xs)[PW + 1] = (T (*)[PW + 1])(shp + PW * (PW + 1));
     T (*Ts)[33] = (T (*)[33])(shp + 2 * PW * (PW + 1));
-    __shared__ T col[2][PW];  // column k of the active block (double-buffered by step parity)
-    __shared__ T piv[PW];     // reciprocal pivots during the sweep, then the square roots
-    __shared__ T rpiv[PW];    // reciprocal square roots of the pivots
+    __shared__ T rdv[PW];  // reciprocal pivots, then the square roots of the pivots
+    __shared__ T rsq[PW];  // reciprocal square roots of the pivots
+    __shared__ int fail;
     int s = fronts[blockIdx.x];
     int ms = D.m[s], w = min(PW, D.ncol[s] - k0);
     T *F = D.F + D.front_off[s];
     T *Inv = D.Inv + D.inv_off[s] + (int64_t)(k0 / PW) * PW * PW;
-    int tid = threadIdx.x, r = tid & (PW - 1), cg = tid >> 6;
-    // thread (r, cg) keeps row r, columns c = cg + 4j, in registers; rows and columns at or beyond the block width
-    // are the identity
-    T R[PW / 4];
-#pragma unroll
-    for (int j = 0; j < PW / 4; j++) {
-        int c = cg + 4 * j;
-        T v = r == c ? T(1) : T(0);
-        if (r < w && c < w && r >= c) v = F[(int64_t)(k0 + c) * ms + k0 + r];
-        R[j] = v;
+    int tid = threadIdx.x, lane = tid & 31, r = tid & (PW - 1), cg = tid >> 6;
+    for (int t = tid; t < PW * PW; t += blockDim.x) {
+        int rr = t % PW, c = t / PW;
+        T v = rr == c ? T(1) : T(0);
+        if (rr < w && c < w && rr >= c) v = F[(int64_t)(k0 + c) * ms + k0 + rr];
+        Ds[rr][c] = v;
+        Xs[rr][c] = T(0);
     }
-    if (cg == 0) {
-        col[0][r] = R[0];
-        if (r == 0) piv[0] = T(1) / R[0];
-    }
-    for (int t = tid; t < PW * (PW + 1); t += blockDim.x) (&Xs[0][0])[t] = T(0);
+    if (tid == 0) fail = -1;
     __syncthreads();
-    // column sweep: each step reads the published column k, updates the registers and publishes column k + 1
-    // (with its pivot's reciprocal, formed by the thread that finishes it); one barrier per column
-    for (int k = 0; k < w; k++) {
-        const T *ck = col[k & 1];
-        T *cn = col[(k + 1) & 1];
-        T d = ck[k];
-        if (!(d > 0)) {
-            if (tid == 0) atomicMin(err, D.c0[s] + k0 + k);
-            return;  // every thread read the same pivot: a uniform exit
-        }
-        T a = ck[r] * piv[k];
-        int jn = (k + 1) >> 2;  // register slot of column k + 1 (owned by cg == (k + 1) & 3)
-        T nxt = T(0);
+    for (int J = 0; J < PW; J += 8) {
+        if (tid < 32) {
+            // lane keeps rows J + lane and J + 32 + lane of the eight columns
+            bool h0 = J + lane < PW, h1 = J + 32 + lane < PW;
+            T a0[8], a1[8];
 #pragma unroll
-        for (int j = 0; j < PW / 4; j++) {
-            int c = cg + 4 * j;
-            T u = ck[c];
-            T v = fma(-a, u, R[j]);
-            R[j] = (c > k && c <= r) ? v : R[j];
-            nxt = j == jn ? R[j] : nxt;
+            for (int q = 0; q < 8; q++) {
+                a0[q] = h0 ? Ds[J + lane][J + q] : T(0);
+                a1[q] = h1 ? Ds[J + 32 + lane][J + q] : T(0);
+            }
+            int bad = -1;
+#pragma unroll
+            for (int kk = 0; kk < 8; kk++) {
+                T d = __shfl_sync(0xffffffffu, a0[kk], kk);
+                if (!(d > 0) && bad < 0) bad = kk;  // the same value in every lane
+                T rd = T(1) / d;
+                T l0 = a0[kk] * rd, l1 = a1[kk] * rd;
+#pragma unroll
+                for (int c = kk + 1; c < 8; c++) {
+                    T acj = __shfl_sync(0xffffffffu, a0[kk], c);  // A[J + c][J + kk]
+                    if (c <= lane) a0[c] = fma(-l0, acj, a0[c]);
+                    a1[c] = fma(-l1, acj, a1[c]);
+                }
+                if (lane == 0) rdv[J + kk] = rd;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (h0 && q <= lane) Ds[J + lane][J + q] = a0[q];
+                if (h1) Ds[J + 32 + lane][J + q] = a1[q];
+            }
+            if (lane == 0 && bad >= 0) fail = J + bad;
         }
-        if (cg == ((k + 1) & 3)) {
-            cn[r] = nxt;
-            if (r == k + 1) piv[r] = T(1) / nxt;
+        __syncthreads();
+        if (fail >= 0) {
+            if (tid == 0) atomicMin(err, D.c0[s] + k0 + fail);
+            return;  // every thread read the same flag: a uniform exit
+        }
+        // trailing block: A[r][c] -= sum_q A[r][J + q] / d_q * A[c][J + q] for J + 8 <= c <= r
+        if (r >= J + 8) {
+            T lr[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) lr[q] = Ds[r][J + q] * rdv[J + q];
+            for (int c = J + 8 + cg; c <= r; c += 4) {
+                T v0 = Ds[r][c], v1 = T(0);
+#pragma unroll
+                for (int q = 0; q < 8; q += 2) {
+                    v0 = fma(-lr[q], Ds[c][J + q], v0);
+                    v1 = fma(-lr[q + 1], Ds[c][J + q + 1], v1);
+                }
+                Ds[r][c] = v0 + v1;
+            }
         }
         __syncthreads();
     }
-    {
-        T dg = T(0);
-#pragma unroll
-        for (int j = 0; j < PW / 4; j++) dg = cg + 4 * j == r ? R[j] : dg;
-        if (cg == (r & 3)) {
-            T q = sqrt(dg);
-            piv[r] = q;
-            rpiv[r] = T(1) / q;
-        }
+    if (tid < PW) {
+        T q = sqrt(Ds[tid][tid]);
+        rdv[tid] = q;
+        rsq[tid] = T(1) / q;
     }
     __syncthreads();
-#pragma unroll
-    for (int j = 0; j < PW / 4; j++) {
-        int c = cg + 4 * j;
-        T v = c == r ? piv[r] : c < r ? R[j] * rpiv[c] : T(0);
-        Ds[r][c] = v;
-        if (r < w && c < w && c <= r) F[(int64_t)(k0 + c) * ms + k0 + r] = v;
-    }
+    for (int c = cg; c <= r; c += 4) Ds[r][c] = c == r ? rdv[r] : Ds[r][c] * rsq[c];
     __syncthreads();
+    for (int t = tid; t < PW * PW; t += blockDim.x) {
+        int rr = t % PW, c = t / PW;
+        if (rr < w && c < w && rr >= c) F[(int64_t)(k0 + c) * ms + k0 + rr] = Ds[rr][c];
+    }
     // 8x8 diagonal blocks: thread (b, j) forward-substitutes column j of block b
     if (tid < PW) {
         int b8 = (tid >> 3) * 8, j = tid & 7;
         T x[8];
 #pragma unroll
         for (int i = 0; i < 8; i++) {
-            T v = i == j ? 1.0 : 0.0;
+            T v = i == j ? T(1) : T(0);
 #pragma unroll
             for (int q = 0; q < i; q++) v = fma(-Ds[b8 + i][b8 + q], x[q], v);
             x[i] = v / Ds[b8 + i][b8 + i];
@@ -161,27 +200,12 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
         for (int i = 0; i < 8; i++) Xs[b8 + i][b8 + j] = x[i];
     }
     __syncthreads();
-    for (int h = 8; h < PW; h *= 2) {
-        // T = L21 X11 for every pair (rows b+h.., columns b..), X11 lower triangular
-        int per = h * h, total = (PW / (2 * h)) * per;
-        for (int t = tid; t < total; t += blockDim.x) {
-            int p = t / per, e = t % per, i = e / h, j = e % h, b = p * 2 * h;
-            T v = 0;
-            for (int q = j; q < h; q++) v = fma(Ds[b + h + i][b + q], Xs[b + q][b + j], v);
-            Ts[p * h + i][j] = v;  // the pairs of one size fill 32 rows
-        }
-        __syncthreads();
-        for (int t = tid; t < total; t += blockDim.x) {
-            int p = t / per, e = t % per, i = e / h, j = e % h, b = p * 2 * h;
-            T v = 0;
-            for (int q = 0; q <= i; q++) v = fma(Xs[b + h + i][b + h + q], Ts[p * h + q][j], v);
-            Xs[b + h + i][b + j] = -v;
-        }
-        __syncthreads();
-    }
+    panel_merge<T, 8>(Ds, Xs, Ts, tid);
+    panel_merge<T, 16>(Ds, Xs, Ts, tid);
+    panel_merge<T, 32>(Ds, Xs, Ts, tid);
     for (int t = tid; t < PW * PW; t += blockDim.x) {
         int i = t % PW, c = t / PW;
-        Inv[t] = (i < w && c < w) ? Xs[i][c] : 0.0;  // column-major, row i
+        Inv[t] = (i < w && c < w) ? Xs[i][c] : T(0);  // column-major, row i
     }
 }
 
