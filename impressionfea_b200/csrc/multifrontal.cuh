@@ -28,6 +28,7 @@ namespace mf {
 
 constexpr int PW = 64;  // panel width
 constexpr int UT = 64;  // update tile
+constexpr int SST = UT + 4;  // row stride of the k-major operand tiles in shared memory (16-byte aligned rows)
 
 template <typename T>
 struct Dev {
@@ -37,6 +38,35 @@ struct Dev {
 };
 
 constexpr int kWideM = 192;  // fronts at least this tall get a full pivot-block inverse and multi-CTA solves
+
+// Four consecutive values from shared memory in one or two vector loads (16-byte aligned addresses).
+__device__ __forceinline__ void lds4(const float *p, float (&v)[4])
+{
+    float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+}
+__device__ __forceinline__ void lds4(const double *p, double (&v)[4])
+{
+    double2 t0 = *reinterpret_cast<const double2 *>(p), t1 = *reinterpret_cast<const double2 *>(p + 2);
+    v[0] = t0.x, v[1] = t0.y, v[2] = t1.x, v[3] = t1.y;
+}
+
+// acc += A^T B over kn steps of two k-major 64-wide tiles: thread (tx, ty) owns rows 4 tx .. 4 tx + 3 of A's
+// columns and columns 4 ty .. 4 ty + 3 of B's, so each step is two or four vector loads for sixteen FMAs.
+template <typename T>
+__device__ __forceinline__ void tile_mma(const T (*A)[SST], const T (*B)[SST], int kn, int tx, int ty, T (&acc)[4][4])
+{
+#pragma unroll 4
+    for (int k = 0; k < kn; k++) {
+        T a[4], b[4];
+        lds4(&A[k][4 * tx], a);
+        lds4(&B[k][4 * ty], b);
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+}
 
 template <typename T>
 static __global__ void k_scatter(int64_t n, const int64_t *__restrict__ dst, const int32_t *__restrict__ src,
@@ -216,8 +246,8 @@ static __global__ void __launch_bounds__(256) k_panel_trsm(Dev<T> D, const int32
 {
     extern __shared__ __align__(16) unsigned char shm_raw[];
     T *shm = (T *)shm_raw;
-    T (*Di)[PW + 1] = (T (*)[PW + 1])shm;
-    T (*Ft)[PW + 1] = (T (*)[PW + 1])(shm + PW * (PW + 1));
+    T (*Ft)[SST] = (T (*)[SST])shm;             // Ft[l][row]
+    T (*Di)[SST] = (T (*)[SST])(shm + PW * SST);  // Di[l][k] = Dinv[k][l]
     int s = fronts[blockIdx.y];
     int ms = D.m[s], w = min(PW, D.ncol[s] - k0);
     int rbeg = k0 + w + blockIdx.x * PW;
@@ -225,29 +255,20 @@ static __global__ void __launch_bounds__(256) k_panel_trsm(Dev<T> D, const int32
     int rows = min(PW, ms - rbeg);
     T *F = D.F + D.front_off[s];
     const T *Inv = D.Inv + D.inv_off[s] + (int64_t)(k0 / PW) * PW * PW;
-    for (int t = threadIdx.x; t < PW * PW; t += blockDim.x) {
-        int c = t / PW, i = t % PW;
-        Di[i][c] = Inv[t];  // column-major inverse: row i, column c
-    }
     for (int t = threadIdx.x; t < w * PW; t += blockDim.x) {
         int l = t / PW, rr = t % PW;
-        Ft[rr][l] = rr < rows ? F[(int64_t)(k0 + l) * ms + rbeg + rr] : 0.0;
+        Di[l][rr] = Inv[t];  // column l of the column-major inverse
+        Ft[l][rr] = rr < rows ? F[(int64_t)(k0 + l) * ms + rbeg + rr] : T(0);
     }
     __syncthreads();
     int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     T acc[4][4];
     for (int a = 0; a < 4; a++)
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
-    for (int l = 0; l < w; l++) {
-        T f[4], d[4];
-        for (int a = 0; a < 4; a++) f[a] = Ft[tx + 16 * a][l];
-        for (int b = 0; b < 4; b++) d[b] = Di[ty + 16 * b][l];
-        for (int a = 0; a < 4; a++)
-            for (int b = 0; b < 4; b++) acc[a][b] = fma(f[a], d[b], acc[a][b]);
-    }
-    for (int a = 0; a < 4; a++)
-        for (int b = 0; b < 4; b++) {
-            int rr = tx + 16 * a, k = ty + 16 * b;
+        for (int b = 0; b < 4; b++) acc[a][b] = T(0);
+    tile_mma<T>(Ft, Di, w, tx, ty, acc);
+    for (int b = 0; b < 4; b++)
+        for (int a = 0; a < 4; a++) {
+            int rr = 4 * tx + a, k = 4 * ty + b;
             if (rr < rows && k < w) F[(int64_t)(k0 + k) * ms + rbeg + rr] = acc[a][b];
         }
 }
@@ -294,8 +315,8 @@ static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev<T> D, const XTask 
 {
     extern __shared__ __align__(16) unsigned char shm_raw[];
     T *shm = (T *)shm_raw;
-    T (*A)[PW + 1] = (T (*)[PW + 1])shm;
-    T (*B)[PW + 1] = (T (*)[PW + 1])(shm + PW * (PW + 1));
+    T (*A)[SST] = (T (*)[SST])shm;             // A[k][r]
+    T (*B)[SST] = (T (*)[SST])(shm + PW * SST);  // B[k][c]
     XTask tk = tasks[blockIdx.x];
     int s = tk.s, bi = tk.bi, bj = tk.bj;
     int ms = D.m[s], nc = D.ncol[s];
@@ -305,7 +326,7 @@ static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev<T> D, const XTask 
     int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     T acc[4][4];
     for (int a = 0; a < 4; a++)
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+        for (int b = 0; b < 4; b++) acc[a][b] = T(0);
     for (int bk = tk.kb0; bk < tk.kb1; bk++) {
         int k0 = bk * PW, wk = min(PW, nc - k0);
         __syncthreads();
@@ -313,27 +334,21 @@ static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev<T> D, const XTask 
             int lo = t % PW, hi = t / PW;  // lo runs along contiguous memory
             // A(r = lo, k = hi): pass 0 L(bi, bk) from the front, pass 1 X(bi, bk)
             bool oka = lo < wr && hi < wk;
-            A[lo][hi] = !oka       ? 0.0
+            A[hi][lo] = !oka       ? T(0)
                         : PASS == 0 ? F[(int64_t)(k0 + hi) * ms + r0 + lo]
                                     : X[(int64_t)(k0 + hi) * nc + r0 + lo];
             if (PASS == 0)  // B(k = lo, c = hi) = X(bk, bj)
-                B[lo][hi] = (lo < wk && hi < wc) ? X[(int64_t)(c0 + hi) * nc + k0 + lo] : 0.0;
+                B[lo][hi] = (lo < wk && hi < wc) ? X[(int64_t)(c0 + hi) * nc + k0 + lo] : T(0);
             else  // B(k = hi, c = lo) = T(bk, bj), stored at X(c0 + c, k0 + k)
-                B[hi][lo] = (hi < wk && lo < wc) ? X[(int64_t)(k0 + hi) * nc + c0 + lo] : 0.0;
+                B[hi][lo] = (hi < wk && lo < wc) ? X[(int64_t)(k0 + hi) * nc + c0 + lo] : T(0);
         }
         __syncthreads();
-        for (int k = 0; k < PW; k++) {
-            T a4[4], b4[4];
-            for (int a = 0; a < 4; a++) a4[a] = A[tx + 16 * a][k];
-            for (int b = 0; b < 4; b++) b4[b] = B[k][ty + 16 * b];
-            for (int a = 0; a < 4; a++)
-                for (int b = 0; b < 4; b++) acc[a][b] = fma(a4[a], b4[b], acc[a][b]);
-        }
+        tile_mma<T>(A, B, PW, tx, ty, acc);
     }
     T *Wt = tk.slot >= 0 ? W + (int64_t)tk.slot * PW * PW : nullptr;
-    for (int a = 0; a < 4; a++)
-        for (int b = 0; b < 4; b++) {
-            int r = tx + 16 * a, c = ty + 16 * b;
+    for (int b = 0; b < 4; b++)
+        for (int a = 0; a < 4; a++) {
+            int r = 4 * tx + a, c = 4 * ty + b;
             if (Wt)
                 Wt[c * PW + r] = acc[a][b];
             else if (r < wr && c < wc)
@@ -489,15 +504,15 @@ static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev<T> D, const int32
     if (lane == 0) x[c0 + j] = v;
 }
 
-// Trailing update of every listed front after panel k0: F22 -= L21 L21^T on 64x64 lower tiles, each thread a
-// 4x4 register block (dynamic shared memory: two 64 x PW panels).
+// Trailing update of every listed front after panel k0: F22 -= L21 L21^T on 64x64 lower tiles (k-major operand
+// tiles in shared memory, each thread a 4x4 register block).
 template <typename T>
 static __global__ void __launch_bounds__(256) k_update(Dev<T> D, const int32_t *__restrict__ fronts, int k0)
 {
     extern __shared__ __align__(16) unsigned char sh_raw[];
     T *sh = (T *)sh_raw;
-    T (*Ai)[PW + 1] = (T (*)[PW + 1])sh;
-    T (*Aj)[PW + 1] = (T (*)[PW + 1])(sh + UT * (PW + 1));
+    T (*Ai)[SST] = (T (*)[SST])sh;
+    T (*Aj)[SST] = (T (*)[SST])(sh + PW * SST);
     int s = fronts[blockIdx.y];
     int ms = D.m[s], w = min(PW, D.ncol[s] - k0), r0 = k0 + w, nt = ms - r0;
     if (nt <= 0) return;
@@ -515,23 +530,18 @@ static __global__ void __launch_bounds__(256) k_update(Dev<T> D, const int32_t *
         for (int q = threadIdx.x; q < UT * w; q += blockDim.x) {
             int rr = q % UT, k = q / UT;
             int gi = ri0 + rr, gj = cj0 + rr;
-            Ai[rr][k] = gi < ms ? F[(int64_t)(k0 + k) * ms + gi] : 0.0;
-            Aj[rr][k] = gj < ms ? F[(int64_t)(k0 + k) * ms + gj] : 0.0;
+            const T *col = F + (int64_t)(k0 + k) * ms;
+            Ai[k][rr] = gi < ms ? col[gi] : T(0);
+            Aj[k][rr] = gj < ms ? col[gj] : T(0);
         }
         __syncthreads();
         T acc[4][4];
         for (int a = 0; a < 4; a++)
-            for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
-        for (int k = 0; k < w; k++) {
-            T ai[4], aj[4];
-            for (int a = 0; a < 4; a++) ai[a] = Ai[tx + 16 * a][k];
-            for (int b = 0; b < 4; b++) aj[b] = Aj[ty + 16 * b][k];
-            for (int a = 0; a < 4; a++)
-                for (int b = 0; b < 4; b++) acc[a][b] = fma(ai[a], aj[b], acc[a][b]);
-        }
-        for (int a = 0; a < 4; a++)
-            for (int b = 0; b < 4; b++) {
-                int gi = ri0 + tx + 16 * a, gj = cj0 + ty + 16 * b;
+            for (int b = 0; b < 4; b++) acc[a][b] = T(0);
+        tile_mma<T>(Ai, Aj, w, tx, ty, acc);
+        for (int b = 0; b < 4; b++)
+            for (int a = 0; a < 4; a++) {
+                int gi = ri0 + 4 * tx + a, gj = cj0 + 4 * ty + b;
                 if (gi < ms && gj < ms && gi >= gj) F[(int64_t)gj * ms + gi] -= acc[a][b];
             }
     }
@@ -964,7 +974,9 @@ public:
             for (int r = 0; r < S.max_rank; r++) {
                 int32_t e0 = S.ext_start[(size_t)l * S.max_rank + r], e1 = S.ext_start[(size_t)l * S.max_rank + r + 1];
                 if (e1 <= e0) continue;
-                dim3 grid(64, e1 - e0);
+                int max_nr = 1;
+                for (int32_t q = e0; q < e1; q++) max_nr = std::max(max_nr, S.m[S.ext_child[q]] - S.ncol[S.ext_child[q]]);
+                dim3 grid(std::min(max_nr, 2048), e1 - e0);  // about one update-matrix column per CTA
                 mf::k_extend<T><<<grid, 128, 0, st>>>(dev_, d_ext_.p + e0, d_par_);
             }
             int q0 = S.level_start[l], q1 = S.level_start[l + 1];
@@ -1097,9 +1109,9 @@ private:
     cudaEvent_t join_ev_ = nullptr;
     cudaGraphExec_t solve_exec_ = nullptr, factor_exec_ = nullptr;
     const double *factor_vals_ = nullptr;
-    static constexpr size_t kUpdateSmem = 2 * mf::UT * (mf::PW + 1) * sizeof(T);
-    static constexpr size_t kPairSmem = 2 * mf::PW * (mf::PW + 1) * sizeof(T);
-    static constexpr size_t kPanelSmem = kPairSmem + 32 * 33 * sizeof(T);
+    static constexpr size_t kUpdateSmem = 2 * mf::PW * mf::SST * sizeof(T);
+    static constexpr size_t kPairSmem = 2 * mf::PW * mf::SST * sizeof(T);
+    static constexpr size_t kPanelSmem = 2 * mf::PW * (mf::PW + 1) * sizeof(T) + 32 * 33 * sizeof(T);
     cudaStream_t st_;
     cusolverSpHandle_t hsp_ = nullptr;
     std::vector<int64_t> inv_off_, xinv_off_;
