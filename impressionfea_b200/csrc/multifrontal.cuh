@@ -37,30 +37,55 @@ struct Dev {
     T *F, *U, *Inv, *Xinv, *Abig;
 };
 
-constexpr int kWideM = 192;  // fronts at least this tall get a full pivot-block inverse and multi-CTA solves
+// Fronts at least this tall get a full pivot-block inverse and multi-CTA solves; shorter ones are eliminated by
+// one CTA each.
+constexpr int kWideM = 192;
 
-// Four consecutive values from shared memory in one or two vector loads (16-byte aligned addresses).
-__device__ __forceinline__ void lds4(const float *p, float (&v)[4])
+// Rows (or columns) of a 64-wide tile owned by thread index t (0..15): four consecutive ones in single precision
+// (one 16-byte shared-memory load), pairs {2t, 2t + 1} and {2t + 32, 2t + 33} in double precision (two 16-byte
+// loads that keep a half-warp on consecutive banks).
+__device__ __forceinline__ int tile_row(float, int t, int a) { return 4 * t + a; }
+__device__ __forceinline__ int tile_row(double, int t, int a) { return 2 * t + (a & 1) + 32 * (a >> 1); }
+__device__ __forceinline__ void lds4(const float *row, int t, float (&v)[4])
 {
-    float4 t = *reinterpret_cast<const float4 *>(p);
-    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+    float4 q = *reinterpret_cast<const float4 *>(row + 4 * t);
+    v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
 }
-__device__ __forceinline__ void lds4(const double *p, double (&v)[4])
+__device__ __forceinline__ void lds4(const double *row, int t, double (&v)[4])
 {
-    double2 t0 = *reinterpret_cast<const double2 *>(p), t1 = *reinterpret_cast<const double2 *>(p + 2);
-    v[0] = t0.x, v[1] = t0.y, v[2] = t1.x, v[3] = t1.y;
+    double2 q0 = *reinterpret_cast<const double2 *>(row + 2 * t), q1 = *reinterpret_cast<const double2 *>(row + 2 * t + 32);
+    v[0] = q0.x, v[1] = q0.y, v[2] = q1.x, v[3] = q1.y;
 }
 
-// acc += A^T B over kn steps of two k-major 64-wide tiles: thread (tx, ty) owns rows 4 tx .. 4 tx + 3 of A's
-// columns and columns 4 ty .. 4 ty + 3 of B's, so each step is two or four vector loads for sixteen FMAs.
+// acc += A^T B over kn steps of two k-major 64-wide tiles: thread (tx, ty) owns rows tile_row(tx, 0..3) of A's
+// columns and tile_row(ty, 0..3) of B's, so each step is two or four vector loads for sixteen FMAs.
+// Asynchronous copy of a 64 x 64 k-major tile into shared memory for a 256-thread CTA (cp.async, no register
+// staging, so all sixteen copies of a thread are in flight together): element (k, r) is src[k * ld + r] when
+// k < kn and r < rn, zero otherwise. tile_wait() completes every copy the thread issued.
+template <typename T>
+__device__ __forceinline__ void tile_fetch(T (*dst)[SST], const T *__restrict__ src, int64_t ld, int kn, int rn)
+{
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        int q = threadIdx.x + 256 * i, r = q & 63, k = q >> 6;
+        bool ok = k < kn && r < rn;
+        const T *g = ok ? src + (int64_t)k * ld + r : src;
+        unsigned sa = (unsigned)__cvta_generic_to_shared(&dst[k][r]);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sa), "l"(g), "n"((int)sizeof(T)),
+                     "r"(ok ? (int)sizeof(T) : 0));
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+}
+__device__ __forceinline__ void tile_wait() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 template <typename T>
 __device__ __forceinline__ void tile_mma(const T (*A)[SST], const T (*B)[SST], int kn, int tx, int ty, T (&acc)[4][4])
 {
 #pragma unroll 4
     for (int k = 0; k < kn; k++) {
         T a[4], b[4];
-        lds4(&A[k][4 * tx], a);
-        lds4(&B[k][4 * ty], b);
+        lds4(A[k], tx, a);
+        lds4(B[k], ty, b);
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -255,11 +280,9 @@ static __global__ void __launch_bounds__(256) k_panel_trsm(Dev<T> D, const int32
     int rows = min(PW, ms - rbeg);
     T *F = D.F + D.front_off[s];
     const T *Inv = D.Inv + D.inv_off[s] + (int64_t)(k0 / PW) * PW * PW;
-    for (int t = threadIdx.x; t < w * PW; t += blockDim.x) {
-        int l = t / PW, rr = t % PW;
-        Di[l][rr] = Inv[t];  // column l of the column-major inverse
-        Ft[l][rr] = rr < rows ? F[(int64_t)(k0 + l) * ms + rbeg + rr] : T(0);
-    }
+    tile_fetch(Di, Inv, PW, w, PW);  // column l of the column-major inverse
+    tile_fetch(Ft, F + (int64_t)k0 * ms + rbeg, ms, w, rows);
+    tile_wait();
     __syncthreads();
     int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     T acc[4][4];
@@ -268,7 +291,7 @@ static __global__ void __launch_bounds__(256) k_panel_trsm(Dev<T> D, const int32
     tile_mma<T>(Ft, Di, w, tx, ty, acc);
     for (int b = 0; b < 4; b++)
         for (int a = 0; a < 4; a++) {
-            int rr = 4 * tx + a, k = 4 * ty + b;
+            int rr = tile_row(T(), tx, a), k = tile_row(T(), ty, b);
             if (rr < rows && k < w) F[(int64_t)(k0 + k) * ms + rbeg + rr] = acc[a][b];
         }
 }
@@ -348,7 +371,7 @@ static __global__ void __launch_bounds__(256) k_xinv_gemm(Dev<T> D, const XTask 
     T *Wt = tk.slot >= 0 ? W + (int64_t)tk.slot * PW * PW : nullptr;
     for (int b = 0; b < 4; b++)
         for (int a = 0; a < 4; a++) {
-            int r = 4 * tx + a, c = 4 * ty + b;
+            int r = tile_row(T(), tx, a), c = tile_row(T(), ty, b);
             if (Wt)
                 Wt[c * PW + r] = acc[a][b];
             else if (r < wr && c < wc)
@@ -526,14 +549,19 @@ static __global__ void __launch_bounds__(256) k_update(Dev<T> D, const int32_t *
         while (ti * (ti + 1) / 2 > t) ti--;
         int tj = t - ti * (ti + 1) / 2;
         int ri0 = r0 + ti * UT, cj0 = r0 + tj * UT;
+        // operand copies and output loads all in flight at once (the output tile belongs to this CTA alone)
         __syncthreads();
-        for (int q = threadIdx.x; q < UT * w; q += blockDim.x) {
-            int rr = q % UT, k = q / UT;
-            int gi = ri0 + rr, gj = cj0 + rr;
-            const T *col = F + (int64_t)(k0 + k) * ms;
-            Ai[k][rr] = gi < ms ? col[gi] : T(0);
-            Aj[k][rr] = gj < ms ? col[gj] : T(0);
-        }
+        tile_fetch(Ai, F + (int64_t)k0 * ms + ri0, ms, w, ms - ri0);
+        tile_fetch(Aj, F + (int64_t)k0 * ms + cj0, ms, w, ms - cj0);
+        T old[4][4];
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+#pragma unroll
+            for (int a = 0; a < 4; a++) {
+                int gi = ri0 + tile_row(T(), tx, a), gj = cj0 + tile_row(T(), ty, b);
+                old[a][b] = (gi < ms && gj < ms && gi >= gj) ? F[(int64_t)gj * ms + gi] : T(0);
+            }
+        tile_wait();
         __syncthreads();
         T acc[4][4];
         for (int a = 0; a < 4; a++)
@@ -541,8 +569,8 @@ static __global__ void __launch_bounds__(256) k_update(Dev<T> D, const int32_t *
         tile_mma<T>(Ai, Aj, w, tx, ty, acc);
         for (int b = 0; b < 4; b++)
             for (int a = 0; a < 4; a++) {
-                int gi = ri0 + 4 * tx + a, gj = cj0 + 4 * ty + b;
-                if (gi < ms && gj < ms && gi >= gj) F[(int64_t)gj * ms + gi] -= acc[a][b];
+                int gi = ri0 + tile_row(T(), tx, a), gj = cj0 + tile_row(T(), ty, b);
+                if (gi < ms && gj < ms && gi >= gj) F[(int64_t)gj * ms + gi] = old[a][b] - acc[a][b];
             }
     }
 }
@@ -712,6 +740,7 @@ public:
     virtual double solve_ms() const = 0;
     virtual int64_t solves() const = 0;
     virtual void set_profile(bool p) = 0;
+    virtual void set_wide_rows(int m) = 0;  // takes effect at the next analysis
     virtual bool analyzed() const = 0;
     virtual bool factored() const = 0;
     virtual int value_bytes() const = 0;
@@ -758,6 +787,7 @@ public:
     int64_t solves() const override { return n_solves_; }
     int value_bytes() const override { return (int)sizeof(T); }
     void set_profile(bool p) override { profile_ = p; }
+    void set_wide_rows(int m) override { wide_m_ = m; }
     int n() const { return sym_.n; }
 
     void analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block) override
@@ -813,7 +843,7 @@ public:
             big_start_[l] = (int32_t)big_list_.size();
             for (int32_t q = S.level_start[l]; q < S.level_start[l + 1]; q++) {
                 int sn = S.level_list[q];
-                if (S.m[sn] >= mf::kWideM) {
+                if (S.m[sn] >= wide_m_) {
                     big_list_.push_back(sn);
                     xinv_off_[sn] = xinv_total;
                     xinv_total += (int64_t)S.ncol[sn] * S.ncol[sn];
@@ -1104,6 +1134,7 @@ private:
     double factor_ms_ = 0, solve_ms_ = 0;
     int64_t n_solves_ = 0;
     bool profile_ = false;
+    int wide_m_ = mf::kWideM;
     cudaStream_t cap_ = nullptr, side_ = nullptr;  // capture stream; side stream of the inverse passes
     std::vector<cudaEvent_t> fork_ev_;
     cudaEvent_t join_ev_ = nullptr;

@@ -64,6 +64,7 @@ struct Forging3D {
     // give up a reused-factor PCG as soon as its contraction rate shows it cannot meet the budget (on with the
     // single-precision factor; off in the reference's FP64 form, whose iteration counts it must reproduce)
     bool pcg_early_abort = false;
+    int wide_rows = mf::kWideM;  // fronts at least this tall use the multi-CTA solve path
     int pcg_failures = 0, pcg_skip = 0, pcg_failures_total = 0;
     // mesh
     TetTopology topo;
@@ -133,6 +134,7 @@ struct Forging3D {
             lin.reset(new MfSolverT<float>(st));
         else
             lin.reset(new MfSolverT<double>(st));
+        lin->set_wide_rows(wide_rows);
         need_analyze = true;
         have_factor = false;
         pcg_skip = pcg_failures = 0;
@@ -742,7 +744,7 @@ struct Forging3D {
         S("front_pool_mb", lin->symbolic().pool * lin->value_bytes() * 1e-6) S("max_front", lin->symbolic().max_m) S("big_fronts", lin->big_fronts())
         S("factor_gpu_ms", lin->factor_ms()) S("solve_gpu_ms", lin->solve_ms()) S("solves", lin->solves())
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
-        S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total)
+        S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows)
 #undef S
         if (nm == "volume") return volume();
         if (nm == "min_quality") return min_quality(d_x);
@@ -755,7 +757,12 @@ struct Forging3D {
         else if (nm == "ds_cur") ds_cur = v;
         else if (nm == "warm") warm = (int)v;
         else if (nm == "profile_solves") lin->set_profile(v != 0);
-        else if (nm == "factor_fp32") {
+        else if (nm == "wide_front_rows") {
+            wide_rows = (int)v;
+            lin->set_wide_rows(wide_rows);
+            need_analyze = true;
+            have_factor = false;
+        } else if (nm == "factor_fp32") {
             use_precision(v != 0);
             pcg_early_abort = v != 0;
         } else if (nm == "pcg_early_abort") pcg_early_abort = v != 0;

@@ -109,9 +109,14 @@ def test_residual_only_assembly(pair):
     _close(gpu.array("r"), ora.array("r"), RTOL_ENERGY, "residual")
 
 
-def test_increments_track_the_oracle():
+@pytest.mark.parametrize("wide_rows", [None, 48])
+def test_increments_track_the_oracle(wide_rows):
+    # wide_rows=48 sends most fronts of this small case through the multi-CTA solve path and the pivot-block
+    # inverses, which the default threshold keeps for the taller fronts of larger meshes
     cfg, mesh, dies = _case(seed=2)
     gpu = Forging3DSolver(cfg, mesh, dies)
+    if wide_rows is not None:
+        gpu.set_scalar("wide_front_rows", wide_rows)
     ora = Oracle3D(cfg, mesh, dies)
     for k in range(4):
         info = gpu.step()
@@ -123,6 +128,8 @@ def test_increments_track_the_oracle():
         _close(gpu.array("x"), ora.array("x"), 1e-9, f"step {k + 1}: coordinates")
         _close(gpu.array("eps"), ora.array("eps"), RTOL_STATE, f"step {k + 1}: effective strain")
         assert abs(gpu.scalar("gap") - ora.scalar("gap")) < 1e-12
+    if wide_rows is not None:
+        assert gpu.scalar("big_fronts") > 0
 
 
 def test_frictionless_upset_load_matches_homogeneous_solution():
