@@ -33,6 +33,8 @@ constexpr int SST = UT + 4;  // row stride of the k-major operand tiles in share
 template <typename T>
 struct Dev {
     const int32_t *ncol, *m, *c0, *idx_start, *idx, *relmap_start, *relmap, *uvec_start, *child_start, *child_list;
+    // per front row (offset idx_start[s] + k): the children's update-vector entries that land on it, child order
+    const int32_t *gat_start, *gat_src;
     const int64_t *front_off, *inv_off, *xinv_off;
     T *F, *U, *Inv, *Xinv, *Abig;
 };
@@ -404,15 +406,11 @@ __device__ __forceinline__ void dev_wide_acc(Dev<T> D, int s, const T *y)
 {
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s];
     T *acc = D.Abig + D.idx_start[s];
-    for (int k = threadIdx.x; k < ms; k += blockDim.x) acc[k] = k < nc ? y[c0 + k] : 0.0;
-    __syncthreads();
-    for (int q = D.child_start[s]; q < D.child_start[s + 1]; q++) {
-        int c = D.child_list[q];
-        int nr = D.m[c] - D.ncol[c];
-        const int32_t *rm = D.relmap + D.relmap_start[c];
-        const T *u = D.U + D.uvec_start[c];
-        for (int i = threadIdx.x; i < nr; i += blockDim.x) acc[rm[i]] -= u[i];
-        __syncthreads();
+    const int32_t *gs = D.gat_start + D.idx_start[s];
+    for (int k = threadIdx.x; k < ms; k += blockDim.x) {
+        T v = k < nc ? y[c0 + k] : T(0);
+        for (int q = gs[k]; q < gs[k + 1]; q++) v -= D.U[D.gat_src[q]];
+        acc[k] = v;
     }
 }
 
@@ -604,16 +602,13 @@ __device__ __forceinline__ void dev_forward(Dev<T> D, int s, T *y)
     const T *F = D.F + D.front_off[s];
     const T *Inv = D.Inv + D.inv_off[s];
     int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    for (int k = tid; k < ms; k += nt) acc[k] = k < nc ? y[c0 + k] : 0.0;
-    __syncthreads();
-    for (int q = D.child_start[s]; q < D.child_start[s + 1]; q++) {
-        int c = D.child_list[q];
-        int nr = D.m[c] - D.ncol[c];
-        const int32_t *rm = D.relmap + D.relmap_start[c];
-        const T *u = D.U + D.uvec_start[c];
-        for (int i = tid; i < nr; i += nt) acc[rm[i]] -= u[i];
-        __syncthreads();
+    const int32_t *gs = D.gat_start + D.idx_start[s];
+    for (int k = tid; k < ms; k += nt) {
+        T v = k < nc ? y[c0 + k] : T(0);
+        for (int q = gs[k]; q < gs[k + 1]; q++) v -= D.U[D.gat_src[q]];
+        acc[k] = v;
     }
+    __syncthreads();
     for (int kb = 0; kb < nc; kb += PW) {
         int w = min(PW, nc - kb);
         const T *I = Inv + (int64_t)(kb / PW) * PW * PW;
@@ -629,6 +624,7 @@ __device__ __forceinline__ void dev_forward(Dev<T> D, int s, T *y)
         // rows below the block
         for (int r = kb + w + tid; r < ms; r += nt) {
             T v = acc[r];
+#pragma unroll 8
             for (int k = 0; k < w; k++) v = fma(-F[(int64_t)(kb + k) * ms + r], yb[k], v);
             acc[r] = v;
         }
@@ -740,7 +736,7 @@ public:
     virtual double solve_ms() const = 0;
     virtual int64_t solves() const = 0;
     virtual void set_profile(bool p) = 0;
-    virtual void set_wide_rows(int m) = 0;  // takes effect at the next analysis
+    virtual void set_wide_rows(int m) = 0;  // height from which fronts take the multi-CTA path (next analysis)
     virtual bool analyzed() const = 0;
     virtual bool factored() const = 0;
     virtual int value_bytes() const = 0;
@@ -816,6 +812,28 @@ public:
         }
         d_cs_.upload(cs, st_);
         d_cl_.upload(cl, st_);
+        {
+            // gather lists: for every front row, its children's update entries in child order (the order the
+            // extend-add of the solves applies them in)
+            int32_t rows = S.idx_start[S.nsuper];
+            std::vector<int32_t> gst(rows + 1, 0), gsrc((size_t)std::max<int64_t>(S.uvec_pool, 1));
+            for (int c = 0; c < S.nsuper; c++) {
+                int p = S.parent[c];
+                if (p < 0) continue;
+                int nr = S.m[c] - S.ncol[c];
+                for (int i = 0; i < nr; i++) gst[S.idx_start[p] + S.relmap[S.relmap_start[c] + i] + 1]++;
+            }
+            for (int32_t k = 0; k < rows; k++) gst[k + 1] += gst[k];
+            std::vector<int32_t> fill(gst.begin(), gst.end() - 1);
+            for (int p = 0; p < S.nsuper; p++)
+                for (int q = cs[p]; q < cs[p + 1]; q++) {
+                    int c = cl[q], nr = S.m[c] - S.ncol[c];
+                    for (int i = 0; i < nr; i++)
+                        gsrc[fill[S.idx_start[p] + S.relmap[S.relmap_start[c] + i]]++] = S.uvec_start[c] + i;
+                }
+            d_gst_.upload(gst, st_);
+            d_gsrc_.upload(gsrc, st_);
+        }
         // per level: fronts sorted by pivot count (descending) so each panel step's active fronts are a prefix
         lvl_sorted_.assign(S.level_list.begin(), S.level_list.end());
         for (int l = 0; l < S.nlevels; l++)
@@ -933,6 +951,7 @@ public:
         dev_.ncol = d_ncol_; dev_.m = d_m_; dev_.c0 = d_c0_; dev_.idx_start = d_idxs_; dev_.idx = d_idx_;
         dev_.relmap_start = d_rms_; dev_.relmap = d_rm_; dev_.uvec_start = d_uvs_; dev_.child_start = d_cs_;
         dev_.child_list = d_cl_; dev_.front_off = d_off_; dev_.F = d_F_; dev_.U = d_U_;
+        dev_.gat_start = d_gst_; dev_.gat_src = d_gsrc_;
         dev_.inv_off = d_inv_off_; dev_.Inv = d_Inv_; dev_.xinv_off = d_xinv_off_; dev_.Xinv = d_Xinv_;
         dev_.Abig = d_Abig_;
         cuda_check(cudaFuncSetAttribute((const void *)mf::k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1153,7 +1172,7 @@ private:
     static constexpr int kXinvChunk = 4;  // tile steps per CTA before a block range is split
     size_t small_smem_ = 8, wide_smem_ = 8, level_smem_ = 8;
     DBuf<int64_t> d_inv_off_, d_xinv_off_;
-    DBuf<int32_t> d_small_, d_big_;
+    DBuf<int32_t> d_small_, d_big_, d_gst_, d_gsrc_;
     DBuf<T> d_Inv_, d_Xinv_, d_Abig_, d_y1_, d_z_;
     cusparseMatDescr_t descr_ = nullptr;
     MfSymbolic sym_;
