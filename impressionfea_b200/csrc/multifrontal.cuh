@@ -420,15 +420,14 @@ __device__ __forceinline__ void dev_wide_acc(Dev<T> D, int s, const T *y)
 // (the longest rows of a triangular operand first).
 constexpr int RT = 16;
 
-// y1 = X acc1 (X lower triangular).
+// y1 = X acc1 (X lower triangular), row tile `tile` (counted from the bottom) of front s.
 template <typename T>
-static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32_t *__restrict__ fronts, T *y, T *Y1)
+__device__ __forceinline__ void dev_wide_fwd_y(Dev<T> D, int s, int tile, T *y, T *Y1)
 {
     __shared__ T part[32][RT + 1];
-    int s = fronts[blockIdx.y];
     int nc = D.ncol[s], c0 = D.c0[s], ntile = (nc + RT - 1) / RT;
-    if ((int)blockIdx.x >= ntile) return;
-    int r0 = (ntile - 1 - blockIdx.x) * RT;
+    if (tile >= ntile) return;
+    int r0 = (ntile - 1 - tile) * RT;
     const T *X = D.Xinv + D.xinv_off[s];
     const T *acc = D.Abig + D.idx_start[s];
     int lane = threadIdx.x & 31, sub = (lane >> 4) + 2 * (threadIdx.x >> 5), rr = lane & (RT - 1);
@@ -448,15 +447,19 @@ static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32
         Y1[D.idx_start[s] + r0 + threadIdx.x] = t;
     }
 }
-
-// update vector t = -acc2 + L21 y1.
 template <typename T>
-static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32_t *__restrict__ fronts, const T *Y1)
+static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32_t *__restrict__ fronts, T *y, T *Y1)
+{
+    dev_wide_fwd_y(D, fronts[blockIdx.y], blockIdx.x, y, Y1);
+}
+
+// update vector t = -acc2 + L21 y1, row tile `tile` of front s.
+template <typename T>
+__device__ __forceinline__ void dev_wide_fwd_t(Dev<T> D, int s, int tile, const T *Y1)
 {
     __shared__ T part[32][RT + 1];
-    int s = fronts[blockIdx.y];
     int ms = D.m[s], nc = D.ncol[s], nr = ms - nc;
-    int i0 = blockIdx.x * RT;
+    int i0 = tile * RT;
     if (i0 >= nr) return;
     const T *F = D.F + D.front_off[s] + nc;
     const T *y1 = Y1 + D.idx_start[s];
@@ -475,6 +478,11 @@ static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32
         int ii = i0 + threadIdx.x;
         D.U[D.uvec_start[s] + ii] = -D.Abig[D.idx_start[s] + nc + ii] + t;
     }
+}
+template <typename T>
+static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32_t *__restrict__ fronts, const T *Y1)
+{
+    dev_wide_fwd_t(D, fronts[blockIdx.y], blockIdx.x, Y1);
 }
 
 // z = y1 - L21^T x2, one warp per pivot column; x2 is gathered into shared memory once per CTA.
@@ -500,17 +508,17 @@ __device__ __forceinline__ void dev_wide_bwd_z(Dev<T> D, int s, int tile, const 
     if (lane == 0) Z[D.idx_start[s] + k] = x[c0 + k] - v;
 }
 
-// x1 = X^T z, one warp per pivot column j (column j of X is contiguous); z is staged in shared memory.
+// x1 = X^T z, one warp per pivot column j (column j of X is contiguous); z is staged in shared memory. Column
+// group `tile` counted from the right end (leftmost, longest columns first).
 template <typename T>
-static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev<T> D, const int32_t *__restrict__ fronts, const T *Z, T *x)
+__device__ __forceinline__ void dev_wide_bwd_x(Dev<T> D, int s, int tile, const T *Z, T *x)
 {
     extern __shared__ __align__(16) unsigned char zs_raw[];
     T *zs = (T *)zs_raw;
-    int s = fronts[blockIdx.y];
     int nc = D.ncol[s], c0 = D.c0[s];
     int nw = blockDim.x >> 5, nblk = (nc + nw - 1) / nw;
-    if ((int)blockIdx.x >= nblk) return;
-    int jbase = (nblk - 1 - blockIdx.x) * nw;  // leftmost (longest) columns first
+    if (tile >= nblk) return;
+    int jbase = (nblk - 1 - tile) * nw;
     const T *z = Z + D.idx_start[s];
     for (int i = jbase + threadIdx.x; i < nc; i += blockDim.x) zs[i - jbase] = z[i];
     __syncthreads();
@@ -523,6 +531,11 @@ static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev<T> D, const int32
     for (int i = j + lane; i < nc; i += 32) v = fma(col[i], zs[i - jbase], v);
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) x[c0 + j] = v;
+}
+template <typename T>
+static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev<T> D, const int32_t *__restrict__ fronts, const T *Z, T *x)
+{
+    dev_wide_bwd_x(D, fronts[blockIdx.y], blockIdx.x, Z, x);
 }
 
 // Trailing update of every listed front after panel k0: F22 -= L21 L21^T on 64x64 lower tiles (k-major operand
