@@ -55,3 +55,22 @@ def test_switching_precision_back_restores_the_fp64_path():
     ora.step()
     assert gpu.scalar("factor_fp32") == 0
     assert abs(info["load"] / ora.scalar("load") - 1) < 1e-6
+
+
+def test_warm_started_fp32_form_meets_the_error_targets_against_a_tight_oracle():
+    # the form bench.py times: extrapolated start (the reference's ExtrapolateStart), Newton tolerance 2e-4, FP32
+    # factor with FP64 refinement; compared with the oracle converged to 1e-6, against the published targets
+    # (ram load within 0.5 %, velocity within 1e-3 relative L2)
+    mesh, dies = upset_case_3d(12.0, 24.0, 1.6, 14.0, seed=4)
+    base = dict(C=150, N=0.1, M=0.12, eps0=0.01, friction=0.4, ram=10, h=1.6, ds=0.32, size=24.0)
+    gpu = Forging3DSolver(Forging3DConfig(**base, tol=2e-4, extrapolate_start=True), mesh, dies)
+    gpu.set_scalar("factor_fp32", 1)
+    ora = Oracle3D(Forging3DConfig(**base, tol=1e-6), mesh, dies)
+    for k in range(5):
+        info = gpu.step()
+        ora.step()
+        le = abs(info["load"] / ora.scalar("load") - 1)
+        ve = _rl2(gpu.array("vg"), ora.array("vg"))
+        assert le < 5e-3, f"step {k + 1}: load error {le:.2e}"
+        assert ve < 1e-3, f"step {k + 1}: velocity rel-L2 {ve:.2e}"
+    assert gpu.scalar("fp32_fallbacks") == 0
