@@ -120,6 +120,10 @@ static __global__ void k_extend(Dev<T> D, const int32_t *__restrict__ children, 
     }
 }
 
+// Correctly rounded reciprocal (CUDA's intrinsic; cheaper than a division on the panel's critical path).
+__device__ __forceinline__ float recip_rn(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double recip_rn(double x) { return __drcp_rn(x); }
+
 // Recursive-doubling merge of the panel inverse at block size H: for every pair of H x H diagonal blocks,
 // X21 = -X22 (L21 X11). The upper triangles of X11 and X22 are zero, so the dot products run over whole blocks.
 template <typename T, int H>
@@ -167,12 +171,20 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
     T *F = D.F + D.front_off[s];
     T *Inv = D.Inv + D.inv_off[s] + (int64_t)(k0 / PW) * PW * PW;
     int tid = threadIdx.x, lane = tid & 31, r = tid & (PW - 1), cg = tid >> 6;
-    for (int t = tid; t < PW * PW; t += blockDim.x) {
-        int rr = t % PW, c = t / PW;
-        T v = rr == c ? T(1) : T(0);
-        if (rr < w && c < w && rr >= c) v = F[(int64_t)(k0 + c) * ms + k0 + rr];
-        Ds[rr][c] = v;
-        Xs[rr][c] = T(0);
+    {
+        T v[16];  // all sixteen loads of a thread in flight before any store
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            int t = tid + 256 * i, rr = t % PW, c = t / PW;
+            v[i] = rr == c ? T(1) : T(0);
+            if (rr < w && c < w && rr >= c) v[i] = F[(int64_t)(k0 + c) * ms + k0 + rr];
+        }
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            int t = tid + 256 * i, rr = t % PW, c = t / PW;
+            Ds[rr][c] = v[i];
+            Xs[rr][c] = T(0);
+        }
     }
     if (tid == 0) fail = -1;
     __syncthreads();
@@ -191,7 +203,7 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
             for (int kk = 0; kk < 8; kk++) {
                 T d = __shfl_sync(0xffffffffu, a0[kk], kk);
                 if (!(d > 0) && bad < 0) bad = kk;  // the same value in every lane
-                T rd = T(1) / d;
+                T rd = recip_rn(d);
                 T l0 = a0[kk] * rd, l1 = a1[kk] * rd;
 #pragma unroll
                 for (int c = kk + 1; c < 8; c++) {
@@ -539,9 +551,11 @@ static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev<T> D, const int32
 }
 
 // Trailing update of every listed front after panel k0: F22 -= L21 L21^T on 64x64 lower tiles (k-major operand
-// tiles in shared memory, each thread a 4x4 register block).
+// tiles in shared memory, each thread a 4x4 register block). part 0: every tile; part 1: the first 64-column block
+// of the trailing matrix (the next panel's columns, which the next panel step needs first); part 2: the tiles
+// right of it (applied on a second stream while the next panel is factorised).
 template <typename T>
-static __global__ void __launch_bounds__(256) k_update(Dev<T> D, const int32_t *__restrict__ fronts, int k0)
+static __global__ void __launch_bounds__(256) k_update(Dev<T> D, const int32_t *__restrict__ fronts, int k0, int part)
 {
     extern __shared__ __align__(16) unsigned char sh_raw[];
     T *sh = (T *)sh_raw;
@@ -552,13 +566,20 @@ static __global__ void __launch_bounds__(256) k_update(Dev<T> D, const int32_t *
     if (nt <= 0) return;
     T *F = D.F + D.front_off[s];
     int nti = (nt + UT - 1) / UT;
-    int ntiles = nti * (nti + 1) / 2;
+    int ntri = part == 2 ? nti - 1 : nti;  // side of the triangle of tiles this part walks
+    int ntiles = part == 1 ? nti : ntri * (ntri + 1) / 2;
     int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        int ti = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-        while ((ti + 1) * (ti + 2) / 2 <= t) ti++;
-        while (ti * (ti + 1) / 2 > t) ti--;
-        int tj = t - ti * (ti + 1) / 2;
+        int ti, tj;
+        if (part == 1) {
+            ti = t, tj = 0;
+        } else {
+            ti = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+            while ((ti + 1) * (ti + 2) / 2 <= t) ti++;
+            while (ti * (ti + 1) / 2 > t) ti--;
+            tj = t - ti * (ti + 1) / 2;
+            if (part == 2) ti++, tj++;
+        }
         int ri0 = r0 + ti * UT, cj0 = r0 + tj * UT;
         // operand copies and output loads all in flight at once (the output tile belongs to this CTA alone)
         __syncthreads();
@@ -767,6 +788,11 @@ public:
         d_err_.resize(2);
         cuda_check(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaStreamCreateWithFlags(&ahead_, cudaStreamNonBlocking), "cudaStreamCreate");
+        int lo = 0;
+        cuda_check(cudaDeviceGetStreamPriorityRange(&lo, &prio_hi_), "cudaDeviceGetStreamPriorityRange");
+        cuda_check(cudaEventCreateWithFlags(&trsm_ev_, cudaEventDisableTiming), "cudaEventCreate");
+        for (auto &e : rest_ev_) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
         cuda_check(cudaEventCreateWithFlags(&join_ev_, cudaEventDisableTiming), "cudaEventCreate");
         for (auto &e : ev_) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
     }
@@ -778,6 +804,10 @@ public:
         for (auto &e : fork_ev_) cudaEventDestroy(e);
         if (join_ev_) cudaEventDestroy(join_ev_);
         if (side_) cudaStreamDestroy(side_);
+        if (trsm_ev_) cudaEventDestroy(trsm_ev_);
+        for (auto &e : rest_ev_)
+            if (e) cudaEventDestroy(e);
+        if (ahead_) cudaStreamDestroy(ahead_);
         if (cap_) cudaStreamDestroy(cap_);
         if (descr_) cusparseDestroyMatDescr(descr_);
         if (hsp_) cusolverSpDestroy(hsp_);
@@ -1043,23 +1073,44 @@ public:
             }
             int q0 = S.level_start[l], q1 = S.level_start[l + 1];
             int maxc = S.ncol[lvl_sorted_[q0]];
-            for (int k0 = 0; k0 < maxc; k0 += mf::PW) {
-                int cnt = 0, maxt = 0, maxr = 0;
+            // panel steps with look-ahead: the trailing update of step p is split into the next panel's columns
+            // (main stream, before panel p + 1) and the rest (second stream, overlapping panel p + 1 and its
+            // solve); the rest of step p - 2 writes the columns of panel p, so it is joined before the next-column
+            // update of step p - 1
+            int prev_cnt = 0, prev_k0 = 0, prev_maxti = 0, np = 0;
+            for (int k0 = 0; k0 < maxc; k0 += mf::PW, np++) {
+                int cnt = 0, maxr = 0, maxti = 0, maxrest = 0;
                 for (int q = q0; q < q1 && S.ncol[lvl_sorted_[q]] > k0; q++) {
                     int sn = lvl_sorted_[q];
                     cnt++;
                     int w = std::min(mf::PW, S.ncol[sn] - k0), nt = S.m[sn] - k0 - w;
                     int nti = (nt + mf::UT - 1) / mf::UT;
-                    maxt = std::max(maxt, nti * (nti + 1) / 2);
+                    maxti = std::max(maxti, nti);
+                    maxrest = std::max(maxrest, nti * (nti - 1) / 2);
                     maxr = std::max(maxr, (nt + mf::PW - 1) / mf::PW);
                 }
-                mf::k_panel<T><<<cnt, 256, kPanelSmem, st>>>(dev_, d_lvl_.p + q0, k0, d_err_);
-                if (maxr > 0) mf::k_panel_trsm<T><<<dim3(maxr, cnt), 256, kPairSmem, st>>>(dev_, d_lvl_.p + q0, k0);
-                if (maxt > 0) {
-                    dim3 grid(std::min(maxt, 4096), cnt);
-                    mf::k_update<T><<<grid, 256, kUpdateSmem, st>>>(dev_, d_lvl_.p + q0, k0);
+                const int32_t *fl = d_lvl_.p + q0;
+                if (np >= 1) {
+                    if (np >= 2) cuda_check(cudaStreamWaitEvent(st, rest_ev_[np % 2], 0), "cudaStreamWaitEvent");
+                    if (prev_maxti > 0)
+                        launch_urgent(mf::k_update<T>, dim3(prev_maxti, prev_cnt), kUpdateSmem, st, dev_, fl, prev_k0, 1);
                 }
+                launch_urgent(mf::k_panel<T>, dim3(cnt), kPanelSmem, st, dev_, fl, k0, (int *)d_err_.p);
+                if (maxr > 0) launch_urgent(mf::k_panel_trsm<T>, dim3(maxr, cnt), kPairSmem, st, dev_, fl, k0);
+                cuda_check(cudaEventRecord(trsm_ev_, st), "cudaEventRecord");
+                cuda_check(cudaStreamWaitEvent(ahead_, trsm_ev_, 0), "cudaStreamWaitEvent");
+                // the rest keeps to about two CTAs per SM, leaving room for the next panel's kernels
+                if (maxrest > 0)
+                    mf::k_update<T><<<dim3(std::min(maxrest, std::max(1, 296 / cnt)), cnt), 256, kUpdateSmem, ahead_>>>(
+                        dev_, fl, k0, 2);
+                cuda_check(cudaEventRecord(rest_ev_[np % 2], ahead_), "cudaEventRecord");
+                prev_cnt = cnt, prev_k0 = k0, prev_maxti = maxti;
             }
+            if (np >= 2) cuda_check(cudaStreamWaitEvent(st, rest_ev_[np % 2], 0), "cudaStreamWaitEvent");
+            if (np >= 1 && prev_maxti > 0)
+                launch_urgent(mf::k_update<T>, dim3(prev_maxti, prev_cnt), kUpdateSmem, st, dev_,
+                              (const int32_t *)(d_lvl_.p + q0), prev_k0, 1);
+            if (np >= 1) cuda_check(cudaStreamWaitEvent(st, rest_ev_[(np - 1) % 2], 0), "cudaStreamWaitEvent");
             if (xinv_pass_start_[l + 1] > xinv_pass_start_[l]) {
                 cuda_check(cudaEventRecord(fork_ev_[l], st), "cudaEventRecord");
                 cuda_check(cudaStreamWaitEvent(side_, fork_ev_[l], 0), "cudaStreamWaitEvent");
@@ -1082,6 +1133,24 @@ public:
             cuda_check(cudaStreamWaitEvent(st, join_ev_, 0), "cudaStreamWaitEvent");
         }
         cuda_check(cudaGetLastError(), "multifrontal factorisation launch");
+    }
+
+    // Launch at the device's greatest stream priority (a kernel-node attribute once captured): the panel chain's
+    // CTAs are scheduled ahead of the look-ahead updates' whenever an SM frees up.
+    template <typename... KArgs, typename... Args>
+    void launch_urgent(void (*kern)(KArgs...), dim3 grid, size_t smem, cudaStream_t st, Args... args)
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributePriority;
+        attr[0].val.priority = prio_hi_;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cuda_check(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...), "cudaLaunchKernelEx");
     }
 
     // x = A^-1 b on the device (b and x may alias). The level sweeps run as one captured CUDA graph on the
@@ -1168,6 +1237,9 @@ private:
     bool profile_ = false;
     int wide_m_ = mf::kWideM;
     cudaStream_t cap_ = nullptr, side_ = nullptr;  // capture stream; side stream of the inverse passes
+    cudaStream_t ahead_ = nullptr;                  // look-ahead stream of the trailing updates
+    cudaEvent_t trsm_ev_ = nullptr, rest_ev_[2] = {nullptr, nullptr};
+    int prio_hi_ = 0;  // greatest stream priority of the device
     std::vector<cudaEvent_t> fork_ev_;
     cudaEvent_t join_ev_ = nullptr;
     cudaGraphExec_t solve_exec_ = nullptr, factor_exec_ = nullptr;
