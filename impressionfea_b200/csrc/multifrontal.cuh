@@ -120,9 +120,22 @@ static __global__ void k_extend(Dev<T> D, const int32_t *__restrict__ children, 
     }
 }
 
-// Correctly rounded reciprocal (CUDA's intrinsic; cheaper than a division on the panel's critical path).
-__device__ __forceinline__ float recip_rn(float x) { return __frcp_rn(x); }
-__device__ __forceinline__ double recip_rn(double x) { return __drcp_rn(x); }
+// Reciprocal of a pivot on the panel's critical path: the fast single-precision intrinsic as the seed, refined by
+// Newton-Raphson steps r <- r (2 - x r), each of which doubles the correct bits (one step for float, two for
+// double); pivots outside the seed's safe range take a plain division.
+__device__ __forceinline__ float recip_rn(float x)
+{
+    if (!(fabsf(x) > 1e-30f && fabsf(x) < 1e30f)) return 1.0f / x;
+    float r = __fdividef(1.0f, x);
+    return r * fmaf(-x, r, 2.0f);
+}
+__device__ __forceinline__ double recip_rn(double x)
+{
+    if (!(fabs(x) > 1e-30 && fabs(x) < 1e30)) return 1.0 / x;
+    double r = (double)__fdividef(1.0f, (float)x);
+    r = r * fma(-x, r, 2.0);
+    return r * fma(-x, r, 2.0);
+}
 
 // Recursive-doubling merge of the panel inverse at block size H: for every pair of H x H diagonal blocks,
 // X21 = -X22 (L21 X11). The upper triangles of X11 and X22 are zero, so the dot products run over whole blocks.
@@ -148,10 +161,60 @@ __device__ __forceinline__ void panel_merge(T (*Ds)[PW + 1], T (*Xs)[PW + 1], T 
     __syncthreads();
 }
 
+// Warp-level L D L^T of the eight columns J .. J + 7 of the panel block over rows J .. 63. Every lane factors the
+// 8 x 8 diagonal block in registers (no shuffles on the pivot chain), then eliminates its own rows J + 8 + lane and
+// J + 40 + lane against it. Reciprocal pivots go to rdv, the lowest failing column to *fail.
+template <typename T>
+__device__ __forceinline__ void panel_factor8(T (*Ds)[PW + 1], T *rdv, int *fail, int J, int lane)
+{
+    T B[8][8], L[8][8], rd[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j <= i; j++) B[i][j] = Ds[J + i][J + j];
+    int bad = -1;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        if (!(B[k][k] > 0) && bad < 0) bad = k;
+        rd[k] = recip_rn(B[k][k]);
+#pragma unroll
+        for (int i = k + 1; i < 8; i++) {
+            L[i][k] = B[i][k] * rd[k];
+#pragma unroll
+            for (int j = k + 1; j <= i; j++) B[i][j] = fma(-L[i][k], B[j][k], B[i][j]);
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        int r = J + 8 + lane + 32 * h;
+        if (r >= PW) continue;
+        T u[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            T v = Ds[r][J + k];
+#pragma unroll
+            for (int j = 0; j < k; j++) v = fma(-u[j], L[k][j], v);
+            u[k] = v;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) Ds[r][J + k] = u[k];
+    }
+    __syncwarp();  // every lane has read the diagonal block
+    if (lane == 0) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+#pragma unroll
+            for (int j = 0; j <= i; j++) Ds[J + i][J + j] = B[i][j];
+            rdv[J + i] = rd[i];
+        }
+    }
+    if (lane == 0 && bad >= 0) *fail = J + bad;
+}
+
 // Panel k0 of every listed front: Cholesky of the diagonal block and the block's inverse (kept for the rows below
 // and for the solves). Blocked L D L^T in shared memory: warp 0 factors eight columns at a time over all rows
-// below them (warp shuffles, no block barrier), then the whole CTA applies the eight columns to the trailing
-// block; the pivot columns are scaled to Cholesky form at the end. Rows and columns at or beyond the block width
+// below them (in registers, no block barrier) while the other warps apply the previous eight to the columns beyond
+// them; the pivot columns are scaled to Cholesky form at the end. Rows and columns at or beyond the block width
 // are the identity. The inverse is built by recursive doubling: the 8x8 diagonal blocks by forward substitution in
 // registers, then merges at sizes 8, 16 and 32. The lowest failing pivot column (new numbering) goes to err.
 // Dynamic shared memory: two 64 x 65 blocks and a 32 x 33 one.
@@ -188,56 +251,48 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
     }
     if (tid == 0) fail = -1;
     __syncthreads();
+    if (tid < 32) panel_factor8(Ds, rdv, &fail, 0, lane);
+    __syncthreads();
+    // look-ahead inside the block: the CTA applies block J to the next eight columns, then warp 0 factors them
+    // while the other warps apply block J to the columns beyond; two barriers per eight columns
     for (int J = 0; J < PW; J += 8) {
-        if (tid < 32) {
-            // lane keeps rows J + lane and J + 32 + lane of the eight columns
-            bool h0 = J + lane < PW, h1 = J + 32 + lane < PW;
-            T a0[8], a1[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                a0[q] = h0 ? Ds[J + lane][J + q] : T(0);
-                a1[q] = h1 ? Ds[J + 32 + lane][J + q] : T(0);
-            }
-            int bad = -1;
-#pragma unroll
-            for (int kk = 0; kk < 8; kk++) {
-                T d = __shfl_sync(0xffffffffu, a0[kk], kk);
-                if (!(d > 0) && bad < 0) bad = kk;  // the same value in every lane
-                T rd = recip_rn(d);
-                T l0 = a0[kk] * rd, l1 = a1[kk] * rd;
-#pragma unroll
-                for (int c = kk + 1; c < 8; c++) {
-                    T acj = __shfl_sync(0xffffffffu, a0[kk], c);  // A[J + c][J + kk]
-                    if (c <= lane) a0[c] = fma(-l0, acj, a0[c]);
-                    a1[c] = fma(-l1, acj, a1[c]);
-                }
-                if (lane == 0) rdv[J + kk] = rd;
-            }
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                if (h0 && q <= lane) Ds[J + lane][J + q] = a0[q];
-                if (h1) Ds[J + 32 + lane][J + q] = a1[q];
-            }
-            if (lane == 0 && bad >= 0) fail = J + bad;
-        }
-        __syncthreads();
         if (fail >= 0) {
             if (tid == 0) atomicMin(err, D.c0[s] + k0 + fail);
             return;  // every thread read the same flag: a uniform exit
         }
-        // trailing block: A[r][c] -= sum_q A[r][J + q] / d_q * A[c][J + q] for J + 8 <= c <= r
-        if (r >= J + 8) {
-            T lr[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) lr[q] = Ds[r][J + q] * rdv[J + q];
-            for (int c = J + 8 + cg; c <= r; c += 4) {
-                T v0 = Ds[r][c], v1 = T(0);
+        if (J + 8 < PW) {
+            // the next eight columns (rows J + 8 .. 63) with block J, spread over the whole CTA
+            for (int e = tid; e < 8 * (PW - J - 8); e += blockDim.x) {
+                int c = J + 8 + (e & 7), rr = J + 8 + (e >> 3);
+                if (c > rr) continue;
+                T v0 = Ds[rr][c], v1 = T(0);
 #pragma unroll
                 for (int q = 0; q < 8; q += 2) {
-                    v0 = fma(-lr[q], Ds[c][J + q], v0);
-                    v1 = fma(-lr[q + 1], Ds[c][J + q + 1], v1);
+                    v0 = fma(-Ds[rr][J + q] * rdv[J + q], Ds[c][J + q], v0);
+                    v1 = fma(-Ds[rr][J + q + 1] * rdv[J + q + 1], Ds[c][J + q + 1], v1);
                 }
-                Ds[r][c] = v0 + v1;
+                Ds[rr][c] = v0 + v1;
+            }
+            __syncthreads();
+        }
+        if (tid < 32) {
+            if (J + 8 < PW) panel_factor8(Ds, rdv, &fail, J + 8, lane);
+        } else {
+            // columns (and rows) J + 16 .. 63: thread u keeps row J + 16 + u % 56 and walks every fourth column
+            int u = tid - 32, rr = J + 16 + u % 56, c0 = J + 16 + u / 56;
+            if (rr < PW) {
+                T lr[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) lr[q] = Ds[rr][J + q] * rdv[J + q];
+                for (int c = c0; c <= rr; c += 4) {
+                    T v0 = Ds[rr][c], v1 = T(0);
+#pragma unroll
+                    for (int q = 0; q < 8; q += 2) {
+                        v0 = fma(-lr[q], Ds[c][J + q], v0);
+                        v1 = fma(-lr[q + 1], Ds[c][J + q + 1], v1);
+                    }
+                    Ds[rr][c] = v0 + v1;
+                }
             }
         }
         __syncthreads();
@@ -263,7 +318,7 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
             T v = i == j ? T(1) : T(0);
 #pragma unroll
             for (int q = 0; q < i; q++) v = fma(-Ds[b8 + i][b8 + q], x[q], v);
-            x[i] = v / Ds[b8 + i][b8 + i];
+            x[i] = v * rsq[b8 + i];  // 1 / L_ii
         }
 #pragma unroll
         for (int i = 0; i < 8; i++) Xs[b8 + i][b8 + j] = x[i];
