@@ -142,21 +142,40 @@ __device__ __forceinline__ double recip_rn(double x)
 template <typename T, int H>
 __device__ __forceinline__ void panel_merge(T (*Ds)[PW + 1], T (*Xs)[PW + 1], T (*Ts)[33], int tid)
 {
-    constexpr int PER = H * H, TOTAL = (PW / (2 * H)) * PER;
-    for (int t = tid; t < TOTAL; t += 256) {
-        int p = t / PER, e = t % PER, i = e / H, j = e % H, b = p * 2 * H;
-        T v = 0;
+    constexpr int PER = H * H, TOTAL = (PW / (2 * H)) * PER, PT = TOTAL / 256;  // entries per thread: 1, 2, 4
+    T v[PT];
 #pragma unroll
-        for (int q = 0; q < H; q++) v = fma(Ds[b + H + i][b + q], Xs[b + q][b + j], v);
-        Ts[p * H + i][j] = v;  // the pairs of one size fill 32 rows
+    for (int k = 0; k < PT; k++) {
+        int t = tid + 256 * k, p = t / PER, e = t % PER, i = e / H, j = e % H, b = p * 2 * H;
+        T a0 = 0, a1 = 0;
+#pragma unroll
+        for (int q = 0; q < H; q += 2) {
+            a0 = fma(Ds[b + H + i][b + q], Xs[b + q][b + j], a0);
+            a1 = fma(Ds[b + H + i][b + q + 1], Xs[b + q + 1][b + j], a1);
+        }
+        v[k] = a0 + a1;
+    }
+#pragma unroll
+    for (int k = 0; k < PT; k++) {
+        int t = tid + 256 * k, p = t / PER, e = t % PER, i = e / H, j = e % H;
+        Ts[p * H + i][j] = v[k];  // the pairs of one size fill 32 rows
     }
     __syncthreads();
-    for (int t = tid; t < TOTAL; t += 256) {
-        int p = t / PER, e = t % PER, i = e / H, j = e % H, b = p * 2 * H;
-        T v = 0;
 #pragma unroll
-        for (int q = 0; q < H; q++) v = fma(Xs[b + H + i][b + H + q], Ts[p * H + q][j], v);
-        Xs[b + H + i][b + j] = -v;
+    for (int k = 0; k < PT; k++) {
+        int t = tid + 256 * k, p = t / PER, e = t % PER, i = e / H, j = e % H, b = p * 2 * H;
+        T a0 = 0, a1 = 0;
+#pragma unroll
+        for (int q = 0; q < H; q += 2) {
+            a0 = fma(Xs[b + H + i][b + H + q], Ts[p * H + q][j], a0);
+            a1 = fma(Xs[b + H + i][b + H + q + 1], Ts[p * H + q + 1][j], a1);
+        }
+        v[k] = a0 + a1;
+    }
+#pragma unroll
+    for (int k = 0; k < PT; k++) {
+        int t = tid + 256 * k, p = t / PER, e = t % PER, i = e / H, j = e % H, b = p * 2 * H;
+        Xs[b + H + i][b + j] = -v[k];
     }
     __syncthreads();
 }
@@ -262,16 +281,24 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
         }
         if (J + 8 < PW) {
             // the next eight columns (rows J + 8 .. 63) with block J, spread over the whole CTA
-            for (int e = tid; e < 8 * (PW - J - 8); e += blockDim.x) {
-                int c = J + 8 + (e & 7), rr = J + 8 + (e >> 3);
-                if (c > rr) continue;
+            T v[2];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {  // 8 x 56 entries at most: two per thread, loads before stores
+                int e = tid + 256 * i, c = J + 8 + (e & 7), rr = J + 8 + (e >> 3);
+                v[i] = T(0);
+                if (rr >= PW || c > rr) continue;
                 T v0 = Ds[rr][c], v1 = T(0);
 #pragma unroll
                 for (int q = 0; q < 8; q += 2) {
                     v0 = fma(-Ds[rr][J + q] * rdv[J + q], Ds[c][J + q], v0);
                     v1 = fma(-Ds[rr][J + q + 1] * rdv[J + q + 1], Ds[c][J + q + 1], v1);
                 }
-                Ds[rr][c] = v0 + v1;
+                v[i] = v0 + v1;
+            }
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                int e = tid + 256 * i, c = J + 8 + (e & 7), rr = J + 8 + (e >> 3);
+                if (rr < PW && c <= rr) Ds[rr][c] = v[i];
             }
             __syncthreads();
         }
@@ -281,17 +308,27 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
             // columns (and rows) J + 16 .. 63: thread u keeps row J + 16 + u % 56 and walks every fourth column
             int u = tid - 32, rr = J + 16 + u % 56, c0 = J + 16 + u / 56;
             if (rr < PW) {
-                T lr[8];
+                T lr[8], v[12];
 #pragma unroll
                 for (int q = 0; q < 8; q++) lr[q] = Ds[rr][J + q] * rdv[J + q];
-                for (int c = c0; c <= rr; c += 4) {
+                // all loads first (at most twelve columns per thread), then the stores
+#pragma unroll
+                for (int i = 0; i < 12; i++) {
+                    int c = c0 + 4 * i;
+                    if (c > rr) break;
                     T v0 = Ds[rr][c], v1 = T(0);
 #pragma unroll
                     for (int q = 0; q < 8; q += 2) {
                         v0 = fma(-lr[q], Ds[c][J + q], v0);
                         v1 = fma(-lr[q + 1], Ds[c][J + q + 1], v1);
                     }
-                    Ds[rr][c] = v0 + v1;
+                    v[i] = v0 + v1;
+                }
+#pragma unroll
+                for (int i = 0; i < 12; i++) {
+                    int c = c0 + 4 * i;
+                    if (c > rr) break;
+                    Ds[rr][c] = v[i];
                 }
             }
         }
@@ -303,11 +340,32 @@ static __global__ void __launch_bounds__(256) k_panel(Dev<T> D, const int32_t *_
         rsq[tid] = T(1) / q;
     }
     __syncthreads();
-    for (int c = cg; c <= r; c += 4) Ds[r][c] = c == r ? rdv[r] : Ds[r][c] * rsq[c];
+    {
+        T v[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            int c = cg + 4 * i;
+            v[i] = c == r ? rdv[r] : c < r ? Ds[r][c] * rsq[c] : T(0);
+        }
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            int c = cg + 4 * i;
+            if (c <= r) Ds[r][c] = v[i];
+        }
+    }
     __syncthreads();
-    for (int t = tid; t < PW * PW; t += blockDim.x) {
-        int rr = t % PW, c = t / PW;
-        if (rr < w && c < w && rr >= c) F[(int64_t)(k0 + c) * ms + k0 + rr] = Ds[rr][c];
+    {
+        T v[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            int t = tid + 256 * i;
+            v[i] = Ds[t % PW][t / PW];
+        }
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            int t = tid + 256 * i, rr = t % PW, c = t / PW;
+            if (rr < w && c < w && rr >= c) F[(int64_t)(k0 + c) * ms + k0 + rr] = v[i];
+        }
     }
     // 8x8 diagonal blocks: thread (b, j) forward-substitutes column j of block b
     if (tid < PW) {
