@@ -181,3 +181,37 @@ def upset_case_3d(R, H, h, shut, seed=0, jitter=0.1):
     mesh = quarter_cylinder(R, H, h, z0=0.0, seed=seed, jitter=jitter, shut=shut)
     dies = (HeightField.flat(0.0, 4 * R + 20), HeightField.flat(shut, 4 * R + 20))
     return mesh, dies
+
+
+def gear_blank_thickness(r, hub_r=15.0, hub_t=22.0, web_t=6.0, rim_in=36.0, rim_r=45.0, rim_t=10.0, flash_t=3.0,
+                         land_ratio=3.0, ramp=1.5):
+    """Part thickness at closure of an axisymmetric gear blank, as a function of the radius: hub (r < hub_r), web
+    of thickness web_t, rim (rim_in < r < rim_r), flash land of gap flash_t and width land_ratio * flash_t, then
+    the gutter (open). Neighbouring levels are joined by linear ramps of width `ramp` (drafts of the impression).
+    The published case gives the hub radius, web thickness, rim radius, flash gap and land ratio; the hub and rim
+    thicknesses and the rim's inner radius are this generator's, chosen so that the cavity up to the land holds
+    about the billet's volume (d40 x h50: 62.8 cm^3) and the excess goes to flash."""
+    r = np.asarray(r, np.float64)
+    land_out = rim_r + land_ratio * flash_t
+    edges = [(hub_r, hub_t, web_t), (rim_in, web_t, rim_t), (rim_r, rim_t, flash_t), (land_out, flash_t, 4 * hub_t)]
+    t = np.full(r.shape, hub_t)
+    for e, a, b in edges:
+        s = np.clip((r - (e - 0.5 * ramp)) / ramp, 0.0, 1.0)
+        t = np.where(r >= e - 0.5 * ramp, a + (b - a) * s, t)
+    return t
+
+
+def gear_blank_case_3d(h, R=20.0, H=50.0, dx=0.5, seed=0, jitter=0.1, **profile):
+    """Closed-die forging of a gear blank (quarter model): billet d = 2R, height H on the bottom die; both dies are
+    height fields sampled at dx from gear_blank_thickness, mirrored about the part's mid-plane, the top die given at
+    its closed position. The billet seats on the highest point of the bottom die under it (z0 = 0) and the top die
+    starts touching it: gap0 = max over billet nodes of (z - top surface)."""
+    zm = 0.5 * float(np.min(gear_blank_thickness(np.linspace(0.0, R, 401), **profile)))  # seat: z0 = 0
+    bottom = HeightField.sample(lambda X, Y: zm - 0.5 * gear_blank_thickness(np.hypot(X, Y), **profile),
+                                -2.0, 70.0, -2.0, 70.0, dx)
+    top = HeightField.sample(lambda X, Y: zm + 0.5 * gear_blank_thickness(np.hypot(X, Y), **profile),
+                             -2.0, 70.0, -2.0, 70.0, dx)
+    mesh = quarter_cylinder(R, H, h, z0=0.0, seed=seed, jitter=jitter)
+    r = np.hypot(mesh.x[:, 0], mesh.x[:, 1])
+    mesh.gap0 = float(np.max(mesh.x[:, 2] - (zm + 0.5 * gear_blank_thickness(r, **profile))))
+    return mesh, (bottom, top)
