@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <climits>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "multifrontal.h"
@@ -720,10 +721,178 @@ static __global__ void __launch_bounds__(256) k_update(Dev<T> D, const int32_t *
     }
 }
 
+// ---------------------------------------------------------------- trailing update on the tensor cores (FP32 factor)
+// The bulk of a single-precision trailing update, C -= A B^T on 128 x 128 lower tiles with K = the panel width, as
+// tcgen05 MMAs of kind::tf32 with the accumulator in tensor memory. Each FP32 operand is split into a TF32 high
+// part and a TF32 remainder, and hi*hi + hi*lo + lo*hi (three MMAs per K step) keeps the products at FP32 accuracy.
+// Operands are staged K-major without swizzle: for every 4-element K chunk, the 128 rows' 16-byte pieces in a row.
+namespace tcu {
+constexpr int TM = 128, TN = 64;
+constexpr int kChunkA = TM * 16, kChunkB = TN * 16;  // bytes of one K chunk of an A (128-row) or B (64-row) tile
+constexpr int kTileA = (PW / 4) * kChunkA, kTileB = (PW / 4) * kChunkB;
+constexpr int kSmem = 2 * kTileA + 2 * kTileB + 64;  // A hi/lo, B hi/lo (96 KB: two CTAs per SM), barrier, address
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ float to_tf32(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+// shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8 rows x 16 B (rows 16 B apart), 8-row
+// groups 128 B apart (stride offset), the two 16-byte K chunks of one MMA a whole chunk (all rows) apart
+// (leading offset); descriptor version 1
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t chunk_bytes)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((chunk_bytes >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((128 >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+// instruction descriptor: D f32, A and B tf32, both K-major, N = 64 (in units of 8), M = 128 (in units of 16)
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+        "l"(da), "l"(db), "r"(kIdesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+// bounded wait on an mbarrier phase (well under a second for an MMA of microseconds): false if it gave up
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (uint32_t it = 0; it < (1u << 16); it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+#define IFEA_TMEM_LD32(taddr, r)                                                                                     \
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"     \
+                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                           \
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),   \
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),           \
+                   "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),         \
+                   "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),         \
+                   "=r"(r[29]), "=r"(r[30]), "=r"(r[31])                                                             \
+                 : "r"(taddr))
+}  // namespace tcu
+
+// The region right of the next panel's columns (rows and columns from r0 + 64 on, r0 = k0 + panel width), as
+// 128 x 64 tiles on or below the diagonal, walked by each CTA in turn; the output tile's old values are loaded
+// while the MMAs run. A wait that gives up records 1 in *err and skips the rest.
+static __global__ void __launch_bounds__(256) k_update_tc(Dev<float> D, const int32_t *__restrict__ fronts, int k0, int *err)
+{
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    float4 *Ahi = (float4 *)tsm, *Alo = Ahi + (PW / 4) * tcu::TM, *Bhi = Alo + (PW / 4) * tcu::TM,
+           *Blo = Bhi + (PW / 4) * tcu::TN;
+    uint64_t *bar = (uint64_t *)(tsm + 2 * tcu::kTileA + 2 * tcu::kTileB);
+    uint32_t *tslot = (uint32_t *)(tsm + 2 * tcu::kTileA + 2 * tcu::kTileB + 16);
+    int s = fronts[blockIdx.y];
+    int ms = D.m[s], w = min(PW, D.ncol[s] - k0), base = k0 + w + PW, nt = ms - base;
+    if (nt <= 0) return;
+    // row tiles of 128, column tiles of 64: row tile ti covers column tiles 0 .. 2 ti + 1
+    int nti = (nt + tcu::TM - 1) / tcu::TM, ntiles = nti * (nti + 1);
+    if ((int)blockIdx.x >= ntiles) return;  // both exits come before the tensor memory is taken
+    float *F = D.F + D.front_off[s];
+    int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tcu::smem_u32(tslot)), "r"(tcu::TN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tcu::smem_u32(bar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+    uint32_t tmem = *tslot, parity = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int ti = (int)((sqrt(4.0 * t + 1.0) - 1.0) * 0.5);  // row tile ti owns tiles ti (ti + 1) .. (ti + 1)(ti + 2) - 1
+        while ((ti + 1) * (ti + 2) <= t) ti++;
+        while (ti * (ti + 1) > t) ti--;
+        int tj = t - ti * (ti + 1);                          // 0 .. 2 ti + 1
+        int ri0 = base + ti * tcu::TM, cj0 = base + tj * tcu::TN;
+        if (cj0 >= ms) continue;         // uniform: the whole CTA skips a tile past the front
+        {
+            // threads 0..127 stage the 128 rows of A, 128..191 the 64 rows of B (the panel's columns of each row)
+            int m = tid < 128 ? tid : tid - 128;
+            if (tid < 128 + tcu::TN) {
+                int row = (tid < 128 ? ri0 : cj0) + m;
+                float4 *hi = tid < 128 ? Ahi : Bhi, *lo = tid < 128 ? Alo : Blo;
+                int rows = tid < 128 ? tcu::TM : tcu::TN;
+                const float *src = F + (int64_t)k0 * ms + row;
+                float v[PW];
+#pragma unroll
+                for (int k = 0; k < PW; k++) v[k] = (k < w && row < ms) ? src[(int64_t)k * ms] : 0.0f;
+#pragma unroll
+                for (int kc = 0; kc < PW / 4; kc++) {
+                    float h[4], l[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        h[j] = tcu::to_tf32(v[4 * kc + j]);
+                        l[j] = tcu::to_tf32(v[4 * kc + j] - h[j]);
+                    }
+                    hi[kc * rows + m] = make_float4(h[0], h[1], h[2], h[3]);
+                    lo[kc * rows + m] = make_float4(l[0], l[1], l[2], l[3]);
+                }
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::);
+            uint32_t ah = tcu::smem_u32(Ahi), al = tcu::smem_u32(Alo), bh = tcu::smem_u32(Bhi), bl = tcu::smem_u32(Blo);
+            int ksteps = (w + 7) / 8;
+            for (int j = 0; j < ksteps; j++) {
+                uint32_t oa = j * 2 * tcu::kChunkA, ob = j * 2 * tcu::kChunkB;
+                tcu::mma(tmem, tcu::sdesc(ah + oa, tcu::kChunkA), tcu::sdesc(bh + ob, tcu::kChunkB), j > 0);
+                tcu::mma(tmem, tcu::sdesc(ah + oa, tcu::kChunkA), tcu::sdesc(bl + ob, tcu::kChunkB), 1);
+                tcu::mma(tmem, tcu::sdesc(al + oa, tcu::kChunkA), tcu::sdesc(bh + ob, tcu::kChunkB), 1);
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(tcu::smem_u32(bar)));
+        }
+        // warp q owns tensor-memory lanes 32 (q % 4) .. + 31 (the tile's rows) and columns 32 (q / 4) .. + 31;
+        // its old output values come in while the MMAs run
+        int lb = 32 * (warp & 3), gi = ri0 + lb + lane, col0 = (warp >> 2) * 32;
+        float old[32];
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            int gj = cj0 + col0 + j;
+            old[j] = (gi < ms && gj < ms && gi >= gj) ? F[(int64_t)gj * ms + gi] : 0.0f;
+        }
+        bool ok = tcu::mbar_wait(tcu::smem_u32(bar), parity);
+        parity ^= 1;
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(err, 1);
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::);
+        {
+            uint32_t r[32];
+            IFEA_TMEM_LD32(tmem + ((uint32_t)lb << 16) + col0, r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                int gj = cj0 + col0 + j;
+                if (gi < ms && gj < ms && gi >= gj) F[(int64_t)gj * ms + gi] = old[j] - __uint_as_float(r[j]);
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::);
+        __syncthreads();
+    }
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcu::TN));
+}
+
 static __global__ void k_init_err(int *err)
 {
     err[0] = INT_MAX;
     err[1] = 0;
+    err[2] = 0;
 }
 
 template <typename T>
@@ -887,6 +1056,8 @@ public:
     virtual bool analyzed() const = 0;
     virtual bool factored() const = 0;
     virtual int value_bytes() const = 0;
+    virtual int64_t tc_launches() const = 0;  // tensor-core trailing-update launches in one factorisation
+    virtual void set_tc(bool on) = 0;         // tensor-core trailing updates on (single precision) or off
 };
 
 template <typename T>
@@ -898,7 +1069,7 @@ public:
         if (cusparseCreateMatDescr(&descr_) != CUSPARSE_STATUS_SUCCESS) throw Failure(IFEA_CUDA_ERROR, "cusparseCreateMatDescr failed");
         cusparseSetMatType(descr_, CUSPARSE_MATRIX_TYPE_GENERAL);
         cusparseSetMatIndexBase(descr_, CUSPARSE_INDEX_BASE_ZERO);
-        d_err_.resize(2);
+        d_err_.resize(4);
         cuda_check(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_check(cudaStreamCreateWithFlags(&ahead_, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -938,6 +1109,12 @@ public:
     double solve_ms() const override { return solve_ms_; }
     int64_t solves() const override { return n_solves_; }
     int value_bytes() const override { return (int)sizeof(T); }
+    int64_t tc_launches() const override { return tc_launches_; }
+    void set_tc(bool on) override
+    {
+        use_tc_ = on && std::is_same<T, float>::value;
+        drop_graphs();
+    }
     void set_profile(bool p) override { profile_ = p; }
     void set_wide_rows(int m) override { wide_m_ = m; }
     int n() const { return sym_.n; }
@@ -1112,6 +1289,9 @@ public:
         dev_.Abig = d_Abig_;
         cuda_check(cudaFuncSetAttribute((const void *)mf::k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kUpdateSmem), "cudaFuncSetAttribute");
+        if constexpr (std::is_same<T, float>::value)
+            cuda_check(cudaFuncSetAttribute((const void *)mf::k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            mf::tcu::kSmem), "cudaFuncSetAttribute");
         cuda_check(cudaFuncSetAttribute((const void *)mf::k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kPanelSmem), "cudaFuncSetAttribute");
         cuda_check(cudaFuncSetAttribute((const void *)mf::k_panel_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1150,11 +1330,12 @@ public:
         cuda_check(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
         cuda_check(cudaGraphLaunch(factor_exec_, st_), "cudaGraphLaunch");
         cuda_check(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
-        int32_t e[2];
+        int32_t e[3];
         cuda_check(cudaMemcpyAsync(e, d_err_.p, sizeof e, cudaMemcpyDeviceToHost, st_), "D2H");
         cuda_check(cudaStreamSynchronize(st_), "cudaStreamSynchronize");
         float ms = 0;
         if (cudaEventElapsedTime(&ms, ev_[0], ev_[1]) == cudaSuccess) factor_ms_ += ms;
+        if (e[2]) throw Failure(IFEA_CUDA_ERROR, "multifrontal factorisation: a tensor-core update timed out");
         if (e[0] != INT_MAX) {
             int row = S.perm[e[0]];
             throw Failure(IFEA_NOT_SPD, "Stiffness matrix not positive definite at equation " + std::to_string(row) +
@@ -1167,6 +1348,7 @@ public:
     {
         const MfSymbolic &S = sym_;
         bool side_used = false;
+        tc_launches_ = 0;
         mf::k_init_err<<<1, 1, 0, st>>>(d_err_);
         for (int l = 0; l < S.nlevels; l++) {
             int64_t p0 = S.level_pool_start[l], p1 = S.level_pool_start[l + 1];
@@ -1192,7 +1374,7 @@ public:
             // update of step p - 1
             int prev_cnt = 0, prev_k0 = 0, prev_maxti = 0, np = 0;
             for (int k0 = 0; k0 < maxc; k0 += mf::PW, np++) {
-                int cnt = 0, maxr = 0, maxti = 0, maxrest = 0;
+                int cnt = 0, maxr = 0, maxti = 0, maxrest = 0, maxtc = 0, maxrows = 0;
                 for (int q = q0; q < q1 && S.ncol[lvl_sorted_[q]] > k0; q++) {
                     int sn = lvl_sorted_[q];
                     cnt++;
@@ -1201,6 +1383,9 @@ public:
                     maxti = std::max(maxti, nti);
                     maxrest = std::max(maxrest, nti * (nti - 1) / 2);
                     maxr = std::max(maxr, (nt + mf::PW - 1) / mf::PW);
+                    int ntc = (std::max(0, nt - mf::PW) + mf::tcu::TM - 1) / mf::tcu::TM;
+                    maxtc = std::max(maxtc, ntc * (ntc + 1));
+                    maxrows = std::max(maxrows, nt - mf::PW);
                 }
                 const int32_t *fl = d_lvl_.p + q0;
                 if (np >= 1) {
@@ -1212,8 +1397,11 @@ public:
                 if (maxr > 0) launch_urgent(mf::k_panel_trsm<T>, dim3(maxr, cnt), kPairSmem, st, dev_, fl, k0);
                 cuda_check(cudaEventRecord(trsm_ev_, st), "cudaEventRecord");
                 cuda_check(cudaStreamWaitEvent(ahead_, trsm_ev_, 0), "cudaStreamWaitEvent");
-                // the rest keeps to about two CTAs per SM, leaving room for the next panel's kernels
-                if (maxrest > 0)
+                // the rest keeps to about two CTAs per SM, leaving room for the next panel's kernels; in single
+                // precision, once it spans kTcRows rows, it runs on the tensor cores
+                if (use_tc_ && maxrows >= kTcRows)
+                    launch_tc(dim3(std::min(maxtc, std::max(1, 296 / cnt)), cnt), fl, k0);
+                else if (maxrest > 0)
                     mf::k_update<T><<<dim3(std::min(maxrest, std::max(1, 296 / cnt)), cnt), 256, kUpdateSmem, ahead_>>>(
                         dev_, fl, k0, 2);
                 cuda_check(cudaEventRecord(rest_ev_[np % 2], ahead_), "cudaEventRecord");
@@ -1246,6 +1434,15 @@ public:
             cuda_check(cudaStreamWaitEvent(st, join_ev_, 0), "cudaStreamWaitEvent");
         }
         cuda_check(cudaGetLastError(), "multifrontal factorisation launch");
+    }
+
+    // The tensor-core trailing update exists for the single-precision factor only.
+    void launch_tc(dim3 grid, const int32_t *fl, int k0)
+    {
+        if constexpr (std::is_same<T, float>::value) {
+            mf::k_update_tc<<<grid, 256, mf::tcu::kSmem, ahead_>>>(dev_, fl, k0, d_err_.p + 2);
+            tc_launches_++;
+        }
     }
 
     // Launch at the device's greatest stream priority (a kernel-node attribute once captured): the panel chain's
@@ -1349,6 +1546,9 @@ private:
     int64_t n_solves_ = 0;
     bool profile_ = false;
     int wide_m_ = mf::kWideM;
+    bool use_tc_ = false;                            // tensor-core trailing updates (single precision, opt-in)
+    int64_t tc_launches_ = 0;                        // tensor-core update launches per factorisation
+    static constexpr int kTcRows = 256;              // trailing rows from which the tensor-core update is used
     cudaStream_t cap_ = nullptr, side_ = nullptr;  // capture stream; side stream of the inverse passes
     cudaStream_t ahead_ = nullptr;                  // look-ahead stream of the trailing updates
     cudaEvent_t trsm_ev_ = nullptr, rest_ev_[2] = {nullptr, nullptr};

@@ -744,7 +744,7 @@ struct Forging3D {
         S("front_pool_mb", lin->symbolic().pool * lin->value_bytes() * 1e-6) S("max_front", lin->symbolic().max_m) S("big_fronts", lin->big_fronts())
         S("factor_gpu_ms", lin->factor_ms()) S("solve_gpu_ms", lin->solve_ms()) S("solves", lin->solves())
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
-        S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows)
+        S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows) S("tc_updates", lin->tc_launches())
 #undef S
         if (nm == "volume") return volume();
         if (nm == "min_quality") return min_quality(d_x);
@@ -757,6 +757,7 @@ struct Forging3D {
         else if (nm == "ds_cur") ds_cur = v;
         else if (nm == "warm") warm = (int)v;
         else if (nm == "profile_solves") lin->set_profile(v != 0);
+        else if (nm == "tc_update") lin->set_tc(v != 0);
         else if (nm == "wide_front_rows") {
             wide_rows = (int)v;
             lin->set_wide_rows(wide_rows);

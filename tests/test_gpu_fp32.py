@@ -25,6 +25,7 @@ def test_fp32_factor_with_refinement_tracks_the_fp64_oracle():
     cfg = Forging3DConfig(C=150, N=0.1, M=0.12, eps0=0.01, friction=0.4, ram=10, h=1.6, ds=0.32, size=24.0, tol=1e-4)
     gpu = Forging3DSolver(cfg, mesh, dies)
     gpu.set_scalar("factor_fp32", 1)
+    gpu.set_scalar("tc_update", 1)  # the tcgen05 trailing update (opt-in) must keep the same accuracy
     ora = Oracle3D(cfg, mesh, dies)
     worst = [0.0, 0.0]
     for k in range(4):
@@ -41,6 +42,7 @@ def test_fp32_factor_with_refinement_tracks_the_fp64_oracle():
     assert gpu.scalar("fp32_fallbacks") == 0
     assert gpu.scalar("refine_its") > 0
     assert gpu.scalar("big_fronts") > 0, "the case must reach the wide-front kernels"
+    assert gpu.scalar("tc_updates") > 0, "the case must reach the tensor-core trailing update"
     print(f"fp32 form: worst load error {worst[0]:.2e}, worst velocity rel-L2 {worst[1]:.2e}")
 
 
