@@ -784,7 +784,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
 // The region right of the next panel's columns (rows and columns from r0 + 64 on, r0 = k0 + panel width), as
 // 128 x 64 tiles on or below the diagonal, walked by each CTA in turn; the output tile's old values are loaded
 // while the MMAs run. A wait that gives up records 1 in *err and skips the rest.
-static __global__ void __launch_bounds__(256) k_update_tc(Dev<float> D, const int32_t *__restrict__ fronts, int k0, int *err)
+static __global__ void __launch_bounds__(256, 2) k_update_tc(Dev<float> D, const int32_t *__restrict__ fronts, int k0, int *err)
 {
     extern __shared__ __align__(1024) unsigned char tsm[];
     float4 *Ahi = (float4 *)tsm, *Alo = Ahi + (PW / 4) * tcu::TM, *Bhi = Alo + (PW / 4) * tcu::TM,
@@ -825,19 +825,21 @@ static __global__ void __launch_bounds__(256) k_update_tc(Dev<float> D, const in
                 float4 *hi = tid < 128 ? Ahi : Bhi, *lo = tid < 128 ? Alo : Blo;
                 int rows = tid < 128 ? tcu::TM : tcu::TN;
                 const float *src = F + (int64_t)k0 * ms + row;
-                float v[PW];
+                for (int g = 0; g < PW; g += 16) {  // sixteen loads in flight at a time keeps the CTA at 128 registers
+                    float v[16];
 #pragma unroll
-                for (int k = 0; k < PW; k++) v[k] = (k < w && row < ms) ? src[(int64_t)k * ms] : 0.0f;
+                    for (int k = 0; k < 16; k++) v[k] = (g + k < w && row < ms) ? src[(int64_t)(g + k) * ms] : 0.0f;
 #pragma unroll
-                for (int kc = 0; kc < PW / 4; kc++) {
-                    float h[4], l[4];
+                    for (int kc = 0; kc < 4; kc++) {
+                        float h[4], l[4];
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        h[j] = tcu::to_tf32(v[4 * kc + j]);
-                        l[j] = tcu::to_tf32(v[4 * kc + j] - h[j]);
+                        for (int j = 0; j < 4; j++) {
+                            h[j] = tcu::to_tf32(v[4 * kc + j]);
+                            l[j] = tcu::to_tf32(v[4 * kc + j] - h[j]);
+                        }
+                        hi[(g / 4 + kc) * rows + m] = make_float4(h[0], h[1], h[2], h[3]);
+                        lo[(g / 4 + kc) * rows + m] = make_float4(l[0], l[1], l[2], l[3]);
                     }
-                    hi[kc * rows + m] = make_float4(h[0], h[1], h[2], h[3]);
-                    lo[kc * rows + m] = make_float4(l[0], l[1], l[2], l[3]);
                 }
             }
         }
@@ -1057,7 +1059,7 @@ public:
     virtual bool factored() const = 0;
     virtual int value_bytes() const = 0;
     virtual int64_t tc_launches() const = 0;  // tensor-core trailing-update launches in one factorisation
-    virtual void set_tc(bool on) = 0;         // tensor-core trailing updates on (single precision) or off
+    virtual void set_tc(bool on, int rows) = 0;  // tensor-core trailing updates (single precision) from `rows` rows
 };
 
 template <typename T>
@@ -1110,9 +1112,10 @@ public:
     int64_t solves() const override { return n_solves_; }
     int value_bytes() const override { return (int)sizeof(T); }
     int64_t tc_launches() const override { return tc_launches_; }
-    void set_tc(bool on) override
+    void set_tc(bool on, int rows) override
     {
         use_tc_ = on && std::is_same<T, float>::value;
+        tc_rows_ = std::max(2 * mf::tcu::TM, rows);
         drop_graphs();
     }
     void set_profile(bool p) override { profile_ = p; }
@@ -1398,8 +1401,8 @@ public:
                 cuda_check(cudaEventRecord(trsm_ev_, st), "cudaEventRecord");
                 cuda_check(cudaStreamWaitEvent(ahead_, trsm_ev_, 0), "cudaStreamWaitEvent");
                 // the rest keeps to about two CTAs per SM, leaving room for the next panel's kernels; in single
-                // precision, once it spans kTcRows rows, it runs on the tensor cores
-                if (use_tc_ && maxrows >= kTcRows)
+                // precision, once it spans tc_rows_ rows, it runs on the tensor cores
+                if (use_tc_ && maxrows >= tc_rows_)
                     launch_tc(dim3(std::min(maxtc, std::max(1, 296 / cnt)), cnt), fl, k0);
                 else if (maxrest > 0)
                     mf::k_update<T><<<dim3(std::min(maxrest, std::max(1, 296 / cnt)), cnt), 256, kUpdateSmem, ahead_>>>(
@@ -1546,9 +1549,9 @@ private:
     int64_t n_solves_ = 0;
     bool profile_ = false;
     int wide_m_ = mf::kWideM;
-    bool use_tc_ = false;                            // tensor-core trailing updates (single precision, opt-in)
+    bool use_tc_ = std::is_same<T, float>::value;  // tensor-core trailing updates (single precision)
     int64_t tc_launches_ = 0;                        // tensor-core update launches per factorisation
-    static constexpr int kTcRows = 256;              // trailing rows from which the tensor-core update is used
+    int tc_rows_ = 1024;                             // trailing rows from which the tensor-core update is used
     cudaStream_t cap_ = nullptr, side_ = nullptr;  // capture stream; side stream of the inverse passes
     cudaStream_t ahead_ = nullptr;                  // look-ahead stream of the trailing updates
     cudaEvent_t trsm_ev_ = nullptr, rest_ev_[2] = {nullptr, nullptr};

@@ -757,7 +757,8 @@ struct Forging3D {
         else if (nm == "ds_cur") ds_cur = v;
         else if (nm == "warm") warm = (int)v;
         else if (nm == "profile_solves") lin->set_profile(v != 0);
-        else if (nm == "tc_update") lin->set_tc(v != 0);
+        else if (nm == "tc_update") lin->set_tc(v != 0, 1024);
+        else if (nm == "tc_rows") lin->set_tc(true, (int)v);
         else if (nm == "wide_front_rows") {
             wide_rows = (int)v;
             lin->set_wide_rows(wide_rows);
