@@ -528,12 +528,12 @@ static __global__ void k_xinv_reduce(Dev<T> D, const XTask *__restrict__ tasks, 
 
 // acc = [b(cols); 0] - children's update vectors (in child order).
 template <typename T>
-__device__ __forceinline__ void dev_wide_acc(Dev<T> D, int s, const T *y)
+__device__ __forceinline__ void dev_wide_acc(Dev<T> D, int s, const T *y, int chunk, int nchunk)
 {
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s];
     T *acc = D.Abig + D.idx_start[s];
     const int32_t *gs = D.gat_start + D.idx_start[s];
-    for (int k = threadIdx.x; k < ms; k += blockDim.x) {
+    for (int k = chunk * blockDim.x + threadIdx.x; k < ms; k += nchunk * blockDim.x) {
         T v = k < nc ? y[c0 + k] : T(0);
         for (int q = gs[k]; q < gs[k + 1]; q++) v -= D.U[D.gat_src[q]];
         acc[k] = v;
@@ -1008,12 +1008,14 @@ __device__ __forceinline__ void dev_backward(Dev<T> D, int s, const T *y, T *x)
 // coming down).
 template <typename T>
 static __global__ void __launch_bounds__(512) k_fwd_level(Dev<T> D, const int32_t *__restrict__ small, int nsmall,
-                                                          const int32_t *__restrict__ big, T *y)
+                                                          const int32_t *__restrict__ big, int nacc, T *y)
 {
-    if ((int)blockIdx.x < nsmall)
+    if ((int)blockIdx.x < nsmall) {
         dev_forward(D, small[blockIdx.x], y);
-    else
-        dev_wide_acc(D, big[blockIdx.x - nsmall], y);
+    } else {
+        int t = blockIdx.x - nsmall;  // nacc CTAs per wide front share its rows
+        dev_wide_acc(D, big[t / nacc], y, t % nacc, nacc);
+    }
 }
 
 template <typename T>
@@ -1502,8 +1504,11 @@ public:
         for (int l = 0; l < S.nlevels; l++) {
             int q0 = small_start_[l], cnt = small_start_[l + 1] - q0;
             int b0 = big_start_[l], bc = big_start_[l + 1] - b0;
+            int nacc = 1;
+            for (int q = b0; q < b0 + bc; q++) nacc = std::max(nacc, (S.m[big_list_[q]] + 511) / 512);
             if (cnt + bc > 0)
-                mf::k_fwd_level<T><<<cnt + bc, 512, small_smem_, st>>>(dev_, d_small_.p + q0, cnt, d_big_.p + b0, d_y_);
+                mf::k_fwd_level<T><<<cnt + bc * nacc, 512, small_smem_, st>>>(dev_, d_small_.p + q0, cnt, d_big_.p + b0,
+                                                                           nacc, d_y_);
             if (bc > 0) {
                 int mnc = 1, mnr = 1;
                 for (int q = b0; q < b0 + bc; q++) {
