@@ -61,9 +61,11 @@ struct Forging3D {
     // single-precision factor refined by FP64 PCG (off: the reference's FP64 direct solve after a factorisation)
     bool factor_fp32 = false;
     int fp32_fallbacks = 0, refine_its = 0;
-    // give up a reused-factor PCG as soon as its contraction rate shows it cannot meet the budget (on with the
-    // single-precision factor; off in the reference's FP64 form, whose iteration counts it must reproduce)
+    // give up a reused-factor PCG as soon as its contraction rate shows it cannot meet the budget, and try a factor
+    // from an earlier increment again only now and then once that failed (on with the single-precision factor;
+    // off in the reference's FP64 form, whose iteration counts it must reproduce)
     bool pcg_early_abort = false;
+    int factor_step = -1, stale_failures = 0;  // increment of the cached factor; failed tries of a stale one
     int wide_rows = mf::kWideM;  // fronts at least this tall use the multi-CTA solve path
     int pcg_failures = 0, pcg_skip = 0, pcg_failures_total = 0;
     // mesh
@@ -411,14 +413,19 @@ struct Forging3D {
     // b -> x; returns 0 for PCG, 1 for a fresh factorisation
     int solve_linear(const double *b, double *x)
     {
+        // single-precision form: a factor from an earlier increment is tried again only every eighth increment
+        // once such a try has failed (tries within the increment of the factor are unaffected)
+        bool stale = have_factor && factor_step != step_index;
+        bool skip_stale = pcg_early_abort && stale && stale_failures > 0 && step_index % 8 != 0;
         if (have_factor && pcg_skip > 0) {
             pcg_skip--;
-        } else if (have_factor) {
+        } else if (have_factor && !skip_stale) {
             int its;
             {
                 PhaseTimer pt(t_pcg);
                 its = pcg(b, x, 1e-7, P.pcg_budget);
             }
+            if (stale) stale_failures = its >= 0 ? 0 : stale_failures + 1;
             if (its >= 0) {
                 pcg_failures = 0;
                 n_pcg++;
@@ -454,6 +461,7 @@ struct Forging3D {
             throw Failure(IFEA_DIVERGED, fmt("Sparse factorisation failed at step %d (GPU multifrontal Cholesky): %s", step_index, f.what()));
         }
         have_factor = true;
+        factor_step = step_index;
         n_fact++;
         if (lin->value_bytes() != 8) {
             // FP64 refinement of the single-precision factor's solution, to the tolerance of the reused-factor PCG
