@@ -183,7 +183,7 @@ FAST_TOL = 2e-4  # Newton tolerance of the timed form: five times tighter than t
 
 
 def closed_die_workload():
-    """Configs[2] geometry: closed-die gear blank (hub r15, web 6 mm, rim r45, flash gap 3 mm, land 3:1) as height
+    """Closed-die gear blank (hub r15, web 6 mm, rim r45, flash gap 3 mm, land 3:1) as height
     fields at dx = 0.5 mm, billet d40 x h50, ~205k tets, C=140, n=0.08, m=0.15, friction 0.3, 200 steps to closure."""
     from impressionfea_b200.config import Forging3DConfig
     from impressionfea_b200.meshes import gear_blank_case_3d, h_for_tets
@@ -202,7 +202,7 @@ def run_closed_die(stream, flush, warmup=2, steps=8):
     from impressionfea_b200.forging3d import Forging3DSolver
 
     cfg, mesh, dies = closed_die_workload()
-    out = {"workload": "closed-die gear blank (configs[2] geometry), increments %d..%d of 200" % (warmup + 1, warmup + steps),
+    out = {"workload": "closed-die gear blank (d40 x h50 billet, ~205k tets), increments %d..%d of 200" % (warmup + 1, warmup + steps),
            "tets": int(mesh.ne), "nodes": int(mesh.nn), "dof": int(3 * mesh.nn)}
     res = {}
     for label, fp32 in (("plain_fp64", False), ("fp32_factor", True)):
