@@ -2,17 +2,21 @@
 #include "mesh3d.h"
 
 #include <algorithm>
-#include <array>
 #include <cmath>
 #include <numeric>
 
 namespace ifea {
 
 namespace {
-struct FaceRec {
-    std::array<int32_t, 3> key;
-    int32_t ins, a, b, c, owner;
+struct FaceKey {
+    int32_t k0, k1, k2, ins;  // sorted node triple, insertion index 4 e + f
 };
+// the four faces of a tet, in the reference's order
+inline void tet_face(const int32_t *tv, int f, int32_t &a, int32_t &b, int32_t &c)
+{
+    static const int8_t F[4][3] = {{0, 2, 1}, {0, 1, 3}, {0, 3, 2}, {1, 2, 3}};
+    a = tv[F[f][0]], b = tv[F[f][1]], c = tv[F[f][2]];
+}
 }  // namespace
 
 std::string TetTopology::build(int nn_, int ne_, const double *x, const int32_t *t, const uint8_t *ox,
@@ -46,44 +50,74 @@ std::string TetTopology::build(int nn_, int ne_, const double *x, const int32_t 
     }
 
     // boundary faces in the Dictionary's insertion order (TetMesh.cs:31-64)
-    std::vector<FaceRec> fr(4 * (size_t)ne);
-    for (int e = 0; e < ne; e++) {
-        int a = tets[4 * e], b = tets[4 * e + 1], c = tets[4 * e + 2], d = tets[4 * e + 3];
-        int f3[4][3] = {{a, c, b}, {a, b, d}, {a, d, c}, {b, c, d}};
+    // a face is on the boundary when no other face has its node set; kept in insertion order
+    std::vector<FaceKey> fr(4 * (size_t)ne);
+    for (int e = 0; e < ne; e++)
         for (int f = 0; f < 4; f++) {
-            FaceRec &r = fr[4 * e + f];
-            r.a = f3[f][0];
-            r.b = f3[f][1];
-            r.c = f3[f][2];
-            r.owner = e;
-            r.ins = 4 * e + f;
-            r.key = {r.a, r.b, r.c};
-            std::sort(r.key.begin(), r.key.end());
+            int32_t a, b, c;
+            tet_face(&tets[4 * (size_t)e], f, a, b, c);
+            if (a > b) std::swap(a, b);
+            if (b > c) std::swap(b, c);
+            if (a > b) std::swap(a, b);
+            fr[4 * (size_t)e + f] = {a, b, c, 4 * e + f};
         }
+    // only the size of each group of equal node sets matters: one (boundary), two (interior) or more (error)
+    std::vector<int32_t> bf;
+    auto group = [&](size_t i, size_t j) {
+        if (j - i == 1) bf.push_back(fr[i].ins);
+        return j - i <= 2;
+    };
+    if (nn < (1 << 21)) {  // node triples packed into one key of 3 x bits(nn) bits, LSD radix sort by 11 bits
+        int nbits = 1;
+        while ((1 << nbits) < nn) nbits++;
+        std::vector<uint64_t> key(fr.size()), key2(fr.size());
+        std::vector<int32_t> ord(fr.size()), ord2(fr.size());
+        for (size_t i = 0; i < fr.size(); i++) {
+            key[i] = ((uint64_t)fr[i].k0 << (2 * nbits)) | ((uint64_t)fr[i].k1 << nbits) | (uint64_t)fr[i].k2;
+            ord[i] = (int32_t)i;
+        }
+        for (int sh = 0; sh < 3 * nbits; sh += 11) {
+            size_t cnt[2049] = {0};
+            for (uint64_t k : key) cnt[((k >> sh) & 2047) + 1]++;
+            for (int b = 0; b < 2048; b++) cnt[b + 1] += cnt[b];
+            for (size_t i = 0; i < key.size(); i++) {
+                size_t d = cnt[(key[i] >> sh) & 2047]++;
+                key2[d] = key[i];
+                ord2[d] = ord[i];
+            }
+            key.swap(key2);
+            ord.swap(ord2);
+        }
+        std::vector<FaceKey> sorted(fr.size());
+        for (size_t i = 0; i < fr.size(); i++) sorted[i] = fr[ord[i]];
+        fr.swap(sorted);
+    } else {
+        std::sort(fr.begin(), fr.end(), [](const FaceKey &p, const FaceKey &q) {
+            if (p.k0 != q.k0) return p.k0 < q.k0;
+            if (p.k1 != q.k1) return p.k1 < q.k1;
+            return p.k2 < q.k2;
+        });
     }
-    std::sort(fr.begin(), fr.end(), [](const FaceRec &p, const FaceRec &q) {
-        return p.key != q.key ? p.key < q.key : p.ins < q.ins;
-    });
-    std::vector<FaceRec> bf;
     for (size_t i = 0; i < fr.size();) {
         size_t j = i + 1;
-        while (j < fr.size() && fr[j].key == fr[i].key) j++;
-        if (j - i > 2) return "Tetrahedral mesh is not manifold (face shared by more than two tets).";
-        if (j - i == 1) bf.push_back(fr[i]);
+        while (j < fr.size() && fr[j].k0 == fr[i].k0 && fr[j].k1 == fr[i].k1 && fr[j].k2 == fr[i].k2) j++;
+        if (!group(i, j)) return "Tetrahedral mesh is not manifold (face shared by more than two tets).";
         i = j;
     }
-    std::sort(bf.begin(), bf.end(), [](const FaceRec &p, const FaceRec &q) { return p.ins < q.ins; });
+    std::sort(bf.begin(), bf.end());
     int nbf = (int)bf.size();
     bface.resize(3 * (size_t)nbf);
     bowner.resize(nbf);
     bsym.resize(nbf);
     is_surface.assign(nn, 0);
     for (int k = 0; k < nbf; k++) {
-        bface[3 * k] = bf[k].a;
-        bface[3 * k + 1] = bf[k].b;
-        bface[3 * k + 2] = bf[k].c;
-        bowner[k] = bf[k].owner;
-        bsym[k] = (ox[bf[k].a] && ox[bf[k].b] && ox[bf[k].c]) || (oy[bf[k].a] && oy[bf[k].b] && oy[bf[k].c]);
+        int32_t a, b, c;
+        tet_face(&tets[4 * (size_t)(bf[k] / 4)], bf[k] % 4, a, b, c);
+        bface[3 * k] = a;
+        bface[3 * k + 1] = b;
+        bface[3 * k + 2] = c;
+        bowner[k] = bf[k] / 4;
+        bsym[k] = (ox[a] && ox[b] && ox[c]) || (oy[a] && oy[b] && oy[c]);
         if (!bsym[k])
             for (int q = 0; q < 3; q++) is_surface[bface[3 * k + q]] = 1;
     }
@@ -112,13 +146,31 @@ std::string TetTopology::build(int nn_, int ne_, const double *x, const int32_t 
     }
     nbr_start.assign(nn + 1, 0);
     nbr.clear();
-    std::vector<int32_t> buf;
+    std::vector<int32_t> buf, mark(nn, -1);
+    std::vector<uint64_t> bits;  // ascending order of a node set through a bitmap over its index window
     max_nbr = 0;
     for (int i = 0; i < nn; i++) {
         buf.clear();
-        for (int32_t n : ring[i]) buf.insert(buf.end(), ring[n].begin(), ring[n].end());
-        std::sort(buf.begin(), buf.end());
-        buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+        int32_t lo = nn, hi = -1;
+        for (int32_t n : ring[i])
+            for (int32_t q : ring[n])
+                if (mark[q] != i) {
+                    mark[q] = i;
+                    buf.push_back(q);
+                    lo = std::min(lo, q);
+                    hi = std::max(hi, q);
+                }
+        if (hi - lo < (1 << 16)) {
+            size_t nw = (size_t)(hi - lo) / 64 + 1;
+            if (bits.size() < nw) bits.resize(nw, 0);
+            for (int32_t q : buf) bits[(q - lo) >> 6] |= 1ull << ((q - lo) & 63);
+            size_t k = 0;
+            for (size_t w = 0; w < nw; w++)
+                for (uint64_t v = bits[w]; v; v &= v - 1) buf[k++] = lo + (int32_t)(64 * w) + __builtin_ctzll(v);
+            std::fill(bits.begin(), bits.begin() + nw, 0);
+        } else {
+            std::sort(buf.begin(), buf.end());
+        }
         nbr.insert(nbr.end(), buf.begin(), buf.end());
         nbr_start[i + 1] = (int32_t)nbr.size();
         max_nbr = std::max<int32_t>(max_nbr, (int32_t)buf.size());
@@ -144,10 +196,20 @@ std::string TetTopology::build(int nn_, int ne_, const double *x, const int32_t 
         const int32_t *it = std::lower_bound(b, e, i);
         return (it != e && *it == i) ? (int32_t)(it - b) : -1;
     };
+    // slot of node i in nbr[j] by a position map of nbr[j] (-1 when absent), column node by column node
+    std::vector<int32_t> pos(nn, -1);
+    auto fill_pos = [&](int j, bool on) {
+        for (int32_t k = nbr_start[j]; k < nbr_start[j + 1]; k++) pos[nbr[k]] = on ? k - nbr_start[j] : -1;
+    };
     e_nbr.assign(16 * (size_t)ne, 0);
-    for (int e = 0; e < ne; e++)
-        for (int a = 0; a < 4; a++)
-            for (int b = 0; b < 4; b++) e_nbr[16 * e + 4 * a + b] = slot(tets[4 * e + b], tets[4 * e + a]);
+    for (int j = 0; j < nn; j++) {
+        fill_pos(j, true);
+        for (int32_t q = nts[j]; q < nts[j + 1]; q++) {
+            int e = ntl[q], b = ntl_local[q];
+            for (int a = 0; a < 4; a++) e_nbr[16 * (size_t)e + 4 * a + b] = pos[tets[4 * e + a]];
+        }
+        fill_pos(j, false);
+    }
     qk.assign(16 * (size_t)ne, 0);
     for (int j = 0; j < nn; j++)
         for (int32_t q = nts[j]; q < nts[j + 1]; q++) {
@@ -184,22 +246,31 @@ std::string TetTopology::build(int nn_, int ne_, const double *x, const int32_t 
     }
     // K_vol gather lists
     kv_start.assign(nn + 1, 0);
-    kv_n.clear();
-    kv_pj.clear();
-    kv_kstart.clear();
-    kv_k.clear();
+    for (int j = 0; j < nn; j++) kv_start[j + 1] = kv_start[j] + (int32_t)ring[j].size();
+    kv_n.resize(kv_start[nn]);
+    kv_pj.resize(kv_start[nn]);
+    kv_kstart.resize(kv_start[nn]);
+    {
+        size_t nk = 0;
+        for (int j = 0; j < nn; j++)
+            for (int32_t n : ring[j]) nk += g_start[n + 1] - g_start[n];
+        kv_k.resize(nk);
+    }
+    int32_t kk = 0;
     for (int j = 0; j < nn; j++) {
+        fill_pos(j, true);
+        int32_t r = kv_start[j];
         for (int32_t n : ring[j]) {
             int32_t pj = -1;
             for (int32_t p = g_start[n]; p < g_start[n + 1]; p++)
                 if (g_node[p] == j) { pj = p; break; }
             if (pj < 0) return "internal error: patch does not contain its ring node";
-            kv_n.push_back(n);
-            kv_pj.push_back(pj);
-            kv_kstart.push_back((int32_t)kv_k.size());
-            for (int32_t p = g_start[n]; p < g_start[n + 1]; p++) kv_k.push_back(slot(j, g_node[p]));
+            kv_n[r] = n;
+            kv_pj[r] = pj;
+            kv_kstart[r++] = kk;
+            for (int32_t p = g_start[n]; p < g_start[n + 1]; p++) kv_k[kk++] = pos[g_node[p]];
         }
-        kv_start[j + 1] = (int32_t)kv_n.size();
+        fill_pos(j, false);
     }
     return "";
 }

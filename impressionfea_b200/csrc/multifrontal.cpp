@@ -39,17 +39,65 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
                                                         gp.data(), gi.data(), nullptr, pnode.data());
         if (st != CUSOLVER_STATUS_SUCCESS) return "METIS ordering failed (cuSOLVER status " + std::to_string((int)st) + ")";
     }
-    std::vector<int32_t> perm0(n), pinv0(n);
-    for (int k = 0; k < nb; k++)
-        for (int c = 0; c < block; c++) perm0[k * block + c] = pnode[k] * block + c;
-    for (int k = 0; k < n; k++) pinv0[perm0[k]] = k;
+    // 1b. Steps 2-6 are structural. When every nonzero of the matrix belongs to a full block x block node block
+    //     (the diagonal blocks included), they run on the node graph and are expanded afterwards: a node's
+    //     columns form a chain in the elimination tree (3k -> 3k + 1 -> 3k + 2 for block 3), the postorder keeps
+    //     them together, column counts are cc(block k + c) = block cc_node(k) - c, and the supernode test and the
+    //     row structures carry over node by node. Otherwise they run on the matrix itself.
+    bool nodal = block > 1, sorted_rows = true;
+    if (nodal) {
+        std::vector<int> nmark(nb, -1), dmark(n, -1);
+        for (int b = 0; b < nb && nodal; b++) {
+            nmark[b] = b;
+            for (int p = gp[b]; p < gp[b + 1]; p++) nmark[gi[p]] = b;
+            int64_t want = (int64_t)block * (gp[b + 1] - gp[b] + 1);
+            for (int c = 0; c < block && nodal; c++) {
+                int d = b * block + c;
+                if (cp[d + 1] - cp[d] != want) {
+                    nodal = false;
+                    break;
+                }
+                // rows in range, in the node's blocks and all distinct (strictly increasing rows need no marks)
+                bool inc = true;
+                for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
+                    int r = ri[p];
+                    if (r < 0 || r >= n || nmark[r / block] != b) {
+                        nodal = false;
+                        break;
+                    }
+                    if (p > cp[d] && r <= ri[p - 1]) inc = false;
+                }
+                sorted_rows = sorted_rows && inc;
+                if (nodal && !inc)
+                    for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
+                        if (dmark[ri[p]] == d) {
+                            nodal = false;
+                            break;
+                        }
+                        dmark[ri[p]] = d;
+                    }
+            }
+        }
+    }
+    const int B = nodal ? block : 1, ns = n / B;  // structural granularity and column count
+    const int32_t *scp = cp, *sri = ri;
+    std::vector<int32_t> perm0(ns), pinv0(ns);
+    if (nodal) {
+        scp = gp.data();
+        sri = gi.data();
+        for (int k = 0; k < nb; k++) perm0[k] = pnode[k];
+    } else {
+        for (int k = 0; k < nb; k++)
+            for (int c = 0; c < block; c++) perm0[k * block + c] = pnode[k] * block + c;
+    }
+    for (int k = 0; k < ns; k++) pinv0[perm0[k]] = k;
 
     // 2. elimination tree of P A P' (Liu's algorithm with path compression)
-    std::vector<int32_t> par(n, -1), anc(n, -1);
-    for (int k = 0; k < n; k++) {
+    std::vector<int32_t> par(ns, -1), anc(ns, -1);
+    for (int k = 0; k < ns; k++) {
         int d = perm0[k];
-        for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
-            int i = pinv0[ri[p]];
+        for (int32_t p = scp[d]; p < scp[d + 1]; p++) {
+            int i = pinv0[sri[p]];
             while (i != -1 && i < k) {
                 int inext = anc[i];
                 anc[i] = k;
@@ -59,8 +107,8 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
         }
     }
     // 3. postorder (children in ascending order)
-    std::vector<int32_t> head(n, -1), next(n, -1), post(n);
-    for (int j = n - 1; j >= 0; j--)
+    std::vector<int32_t> head(ns, -1), next(ns, -1), post(ns);
+    for (int j = ns - 1; j >= 0; j--)
         if (par[j] != -1) {
             next[j] = head[par[j]];
             head[par[j]] = j;
@@ -68,7 +116,7 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
     {
         std::vector<int32_t> stack;
         int k = 0;
-        for (int j = 0; j < n; j++) {
+        for (int j = 0; j < ns; j++) {
             if (par[j] != -1) continue;
             stack.push_back(j);
             while (!stack.empty()) {
@@ -83,26 +131,26 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
                 }
             }
         }
-        if (k != n) return "internal error: elimination tree postorder incomplete";
+        if (k != ns) return "internal error: elimination tree postorder incomplete";
     }
-    perm.resize(n);
-    pinv.resize(n);
-    std::vector<int32_t> postinv(n);
-    for (int k = 0; k < n; k++) postinv[post[k]] = k;
-    for (int k = 0; k < n; k++) perm[k] = perm0[post[k]];
-    for (int k = 0; k < n; k++) pinv[perm[k]] = k;
-    std::vector<int32_t> parent_c(n);
-    for (int k = 0; k < n; k++) parent_c[k] = par[post[k]] < 0 ? -1 : postinv[par[post[k]]];
+    perm.resize(ns);
+    pinv.resize(ns);
+    std::vector<int32_t> postinv(ns);
+    for (int k = 0; k < ns; k++) postinv[post[k]] = k;
+    for (int k = 0; k < ns; k++) perm[k] = perm0[post[k]];
+    for (int k = 0; k < ns; k++) pinv[perm[k]] = k;
+    std::vector<int32_t> parent_c(ns);
+    for (int k = 0; k < ns; k++) parent_c[k] = par[post[k]] < 0 ? -1 : postinv[par[post[k]]];
 
     // 4. column counts of L by row subtrees (ereach)
-    std::vector<int64_t> cc(n, 1);
+    std::vector<int64_t> cc(ns, 1);
     {
-        std::vector<int32_t> mark(n, -1);
-        for (int k = 0; k < n; k++) {
+        std::vector<int32_t> mark(ns, -1);
+        for (int k = 0; k < ns; k++) {
             mark[k] = k;
             int d = perm[k];
-            for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
-                int i = pinv[ri[p]];
+            for (int32_t p = scp[d]; p < scp[d + 1]; p++) {
+                int i = pinv[sri[p]];
                 if (i >= k) continue;
                 while (mark[i] != k) {
                     cc[i]++;
@@ -114,16 +162,16 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
         }
     }
     // 5. supernodes: k joins k-1's supernode when struct(L_{k-1}) = {k-1} u struct(L_k)
-    std::vector<int32_t> sn_of(n);
+    std::vector<int32_t> sn_of(ns);
     c0.clear();
-    for (int k = 0; k < n; k++) {
+    for (int k = 0; k < ns; k++) {
         bool join = k > 0 && parent_c[k - 1] == k && cc[k - 1] == cc[k] + 1;
         if (!join) c0.push_back(k);
         sn_of[k] = (int)c0.size() - 1;
     }
     nsuper = (int)c0.size();
     ncol.resize(nsuper);
-    for (int s = 0; s < nsuper; s++) ncol[s] = (s + 1 < nsuper ? c0[s + 1] : n) - c0[s];
+    for (int s = 0; s < nsuper; s++) ncol[s] = (s + 1 < nsuper ? c0[s + 1] : ns) - c0[s];
     parent.assign(nsuper, -1);
     for (int s = 0; s < nsuper; s++) {
         int last = c0[s] + ncol[s] - 1;
@@ -135,14 +183,14 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
     for (int s = 0; s < nsuper; s++)
         if (parent[s] >= 0) kids[parent[s]].push_back(s);
     {
-        std::vector<int32_t> mark(n, -1);
+        std::vector<int32_t> mark(ns, -1);
         for (int s = 0; s < nsuper; s++) {
             int first = c0[s], end = c0[s] + ncol[s];
             auto &v = strc[s];
             for (int j = first; j < end; j++) {
                 int d = perm[j];
-                for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
-                    int i = pinv[ri[p]];
+                for (int32_t p = scp[d]; p < scp[d + 1]; p++) {
+                    int i = pinv[sri[p]];
                     if (i >= end && mark[i] != s) {
                         mark[i] = s;
                         v.push_back(i);
@@ -157,6 +205,22 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
                     }
             std::sort(v.begin(), v.end());
             if ((int64_t)v.size() + ncol[s] != cc[first]) return "internal error: supernode structure does not match the column counts";
+        }
+    }
+    if (B > 1) {  // node numbering -> equation numbering
+        std::vector<int32_t> pn(perm);
+        perm.resize(n);
+        pinv.resize(n);
+        for (int k = 0; k < ns; k++)
+            for (int c = 0; c < B; c++) perm[k * B + c] = pn[k] * B + c;
+        for (int k = 0; k < n; k++) pinv[perm[k]] = k;
+        for (int s = 0; s < nsuper; s++) {
+            c0[s] *= B;
+            ncol[s] *= B;
+            std::vector<int32_t> v(strc[s].size() * B);
+            for (size_t k = 0; k < strc[s].size(); k++)
+                for (int c = 0; c < B; c++) v[k * B + c] = strc[s][k] * B + c;
+            strc[s] = std::move(v);
         }
     }
     // 6b. relaxed amalgamation: merge a supernode into its parent when it is the parent's contiguous (last) child
@@ -262,39 +326,57 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
     }
     uvec_pool = uvec_start[nsuper];
     relmap.assign(relmap_start[nsuper], 0);
-    for (int s = 0; s < nsuper; s++) {
-        int p = parent[s];
-        if (p < 0) {
-            if (!strc[s].empty()) return "internal error: a root supernode has off-diagonal rows";
-            continue;
-        }
-        const int32_t *pb = idx.data() + idx_start[p], *pe = pb + m[p];
-        for (size_t k = 0; k < strc[s].size(); k++) {
-            const int32_t *it = std::lower_bound(pb, pe, strc[s][k]);
-            if (it == pe || *it != strc[s][k]) return "internal error: child row missing from the parent front";
-            relmap[relmap_start[s] + k] = (int32_t)(it - pb);
-        }
+    std::vector<int32_t> pos(n, -1);  // row -> position in the front at hand (reset after each front)
+    for (int p = 0; p < nsuper; p++) {
+        if (parent[p] < 0 && !strc[p].empty()) return "internal error: a root supernode has off-diagonal rows";
+        if (kids[p].empty()) continue;
+        const int32_t *pb = idx.data() + idx_start[p];
+        for (int k = 0; k < m[p]; k++) pos[pb[k]] = k;
+        for (int s : kids[p])
+            for (size_t k = 0; k < strc[s].size(); k++) {
+                int32_t q = pos[strc[s][k]];
+                if (q < 0) return "internal error: child row missing from the parent front";
+                relmap[relmap_start[s] + k] = q;
+            }
+        for (int k = 0; k < m[p]; k++) pos[pb[k]] = -1;
     }
     // original values -> fronts, grouped by level
     a_dst.clear();
     a_src.clear();
+    a_dst.reserve(((size_t)cp[n] + n) / 2);
+    a_src.reserve(((size_t)cp[n] + n) / 2);
     a_level_start.assign(nlevels + 1, 0);
     for (int l = 0; l < nlevels; l++) {
         a_level_start[l] = (int32_t)a_src.size();
         for (int32_t q = level_start[l]; q < level_start[l + 1]; q++) {
             int s = level_list[q];
-            const int32_t *ib = idx.data() + idx_start[s], *ie = ib + m[s];
+            const int32_t *ib = idx.data() + idx_start[s];
+            for (int k = 0; k < m[s]; k++) pos[ib[k]] = k;
             for (int j = c0[s]; j < c0[s] + ncol[s]; j++) {
                 int d = perm[j];
+                int64_t base = front_off[s] + (int64_t)(j - c0[s]) * m[s];
+                if (nodal && sorted_rows) {
+                    // rows come in whole node blocks, consecutive in the new numbering and in the front
+                    for (int32_t p = cp[d]; p < cp[d + 1]; p += B) {
+                        int i0 = pinv[ri[p]];
+                        if (i0 + B - 1 < j) continue;
+                        if (pos[i0] < 0) return "internal error: matrix entry outside its front";
+                        for (int r = std::max(0, j - i0); r < B; r++) {
+                            a_dst.push_back(base + pos[i0] + r);
+                            a_src.push_back(p + r);
+                        }
+                    }
+                    continue;
+                }
                 for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
                     int i = pinv[ri[p]];
                     if (i < j) continue;
-                    const int32_t *it = std::lower_bound(ib, ie, i);
-                    if (it == ie || *it != i) return "internal error: matrix entry outside its front";
-                    a_dst.push_back(front_off[s] + (int64_t)(j - c0[s]) * m[s] + (it - ib));
+                    if (pos[i] < 0) return "internal error: matrix entry outside its front";
+                    a_dst.push_back(base + pos[i]);
                     a_src.push_back(p);
                 }
             }
+            for (int k = 0; k < m[s]; k++) pos[ib[k]] = -1;
         }
     }
     a_level_start[nlevels] = (int32_t)a_src.size();

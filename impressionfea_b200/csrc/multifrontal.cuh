@@ -15,6 +15,7 @@
 #include <cusparse.h>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <string>
 #include <type_traits>
@@ -1062,6 +1063,16 @@ public:
     virtual int value_bytes() const = 0;
     virtual int64_t tc_launches() const = 0;  // tensor-core trailing-update launches in one factorisation
     virtual void set_tc(bool on, int rows) = 0;  // tensor-core trailing updates (single precision) from `rows` rows
+    // host seconds spent in: 0 symbolic analysis, 1 its device tables, 2 the factorisation graph, 3 the solve graph
+    virtual double setup_s(int part) const = 0;
+};
+
+// Adds the host time of its scope to a counter.
+struct HostClock {
+    double &acc;
+    std::chrono::steady_clock::time_point t0;
+    explicit HostClock(double &a) : acc(a), t0(std::chrono::steady_clock::now()) {}
+    ~HostClock() { acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
 };
 
 template <typename T>
@@ -1110,6 +1121,7 @@ public:
     const MfSymbolic &symbolic() const override { return sym_; }
     int big_fronts() const override { return (int)big_list_.size(); }
     double factor_ms() const override { return factor_ms_; }
+    double setup_s(int part) const override { return setup_s_[part]; }
     double solve_ms() const override { return solve_ms_; }
     int64_t solves() const override { return n_solves_; }
     int value_bytes() const override { return (int)sizeof(T); }
@@ -1128,8 +1140,13 @@ public:
     {
         analyzed_ = factored_ = false;
         drop_graphs();
-        std::string e = sym_.analyze(n, col_ptr, row_idx, block, hsp_, descr_);
+        std::string e;
+        {
+            HostClock hc(setup_s_[0]);
+            e = sym_.analyze(n, col_ptr, row_idx, block, hsp_, descr_);
+        }
         if (!e.empty()) throw Failure(IFEA_INPUT_INVALID, e);
+        HostClock hc(setup_s_[1]);
         const MfSymbolic &S = sym_;
 
         d_ncol_.upload(S.ncol, st_); d_m_.upload(S.m, st_); d_c0_.upload(S.c0, st_); d_idxs_.upload(S.idx_start, st_);
@@ -1321,6 +1338,7 @@ public:
         factored_ = false;
         const MfSymbolic &S = sym_;
         if (!factor_exec_ || factor_vals_ != d_full_vals) {
+            HostClock hc(setup_s_[2]);
             if (factor_exec_) cudaGraphExecDestroy(factor_exec_);
             factor_exec_ = nullptr;
             cudaGraph_t g = nullptr;
@@ -1476,6 +1494,7 @@ public:
         const MfSymbolic &S = sym_;
         int n = S.n, g = std::max(1, std::min((n + 255) / 256, 4 * 148));
         if (!solve_exec_) {
+            HostClock hc(setup_s_[3]);
             cudaGraph_t gr = nullptr;
             cuda_check(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
             enqueue_sweeps(cap_);
@@ -1550,7 +1569,7 @@ private:
         factor_vals_ = nullptr;
     }
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
-    double factor_ms_ = 0, solve_ms_ = 0;
+    double factor_ms_ = 0, solve_ms_ = 0, setup_s_[4] = {0, 0, 0, 0};
     int64_t n_solves_ = 0;
     bool profile_ = false;
     int wide_m_ = mf::kWideM;
