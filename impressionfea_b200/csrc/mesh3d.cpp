@@ -136,24 +136,38 @@ std::string TetTopology::build(int nn_, int ne_, const double *x, const int32_t 
     }
 
     // patches (one ring, sorted) and the two-ring pattern
-    std::vector<std::vector<int32_t>> ring(nn);
+    std::vector<int32_t> ring_start(nn + 1, 0), ring_list, mark(nn, -1);
+    ring_list.reserve(16 * (size_t)nn);
     for (int n = 0; n < nn; n++) {
-        auto &r = ring[n];
         for (int32_t q = nts[n]; q < nts[n + 1]; q++)
-            for (int a = 0; a < 4; a++) r.push_back(tets[4 * ntl[q] + a]);
-        std::sort(r.begin(), r.end());
-        r.erase(std::unique(r.begin(), r.end()), r.end());
+            for (int a = 0; a < 4; a++) {
+                int32_t v = tets[4 * ntl[q] + a];
+                if (mark[v] != n) {
+                    mark[v] = n;
+                    ring_list.push_back(v);
+                }
+            }
+        std::sort(ring_list.begin() + ring_start[n], ring_list.end());
+        ring_start[n + 1] = (int32_t)ring_list.size();
     }
+    struct Span {
+        const int32_t *b, *e;
+        const int32_t *begin() const { return b; }
+        const int32_t *end() const { return e; }
+        size_t size() const { return (size_t)(e - b); }
+    };
+    auto ring = [&](int i) { return Span{ring_list.data() + ring_start[i], ring_list.data() + ring_start[i + 1]}; };
     nbr_start.assign(nn + 1, 0);
     nbr.clear();
-    std::vector<int32_t> buf, mark(nn, -1);
+    std::vector<int32_t> buf;
+    std::fill(mark.begin(), mark.end(), -1);
     std::vector<uint64_t> bits;  // ascending order of a node set through a bitmap over its index window
     max_nbr = 0;
     for (int i = 0; i < nn; i++) {
         buf.clear();
         int32_t lo = nn, hi = -1;
-        for (int32_t n : ring[i])
-            for (int32_t q : ring[n])
+        for (int32_t n : ring(i))
+            for (int32_t q : ring(n))
                 if (mark[q] != i) {
                     mark[q] = i;
                     buf.push_back(q);
@@ -246,21 +260,21 @@ std::string TetTopology::build(int nn_, int ne_, const double *x, const int32_t 
     }
     // K_vol gather lists
     kv_start.assign(nn + 1, 0);
-    for (int j = 0; j < nn; j++) kv_start[j + 1] = kv_start[j] + (int32_t)ring[j].size();
+    for (int j = 0; j < nn; j++) kv_start[j + 1] = kv_start[j] + (int32_t)ring(j).size();
     kv_n.resize(kv_start[nn]);
     kv_pj.resize(kv_start[nn]);
     kv_kstart.resize(kv_start[nn]);
     {
         size_t nk = 0;
         for (int j = 0; j < nn; j++)
-            for (int32_t n : ring[j]) nk += g_start[n + 1] - g_start[n];
+            for (int32_t n : ring(j)) nk += g_start[n + 1] - g_start[n];
         kv_k.resize(nk);
     }
     int32_t kk = 0;
     for (int j = 0; j < nn; j++) {
         fill_pos(j, true);
         int32_t r = kv_start[j];
-        for (int32_t n : ring[j]) {
+        for (int32_t n : ring(j)) {
             int32_t pj = -1;
             for (int32_t p = g_start[n]; p < g_start[n + 1]; p++)
                 if (g_node[p] == j) { pj = p; break; }

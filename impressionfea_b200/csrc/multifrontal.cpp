@@ -5,7 +5,11 @@
 #include <cusparse.h>
 
 #include <algorithm>
+#include <atomic>
+#include <climits>
+#include <functional>
 #include <numeric>
+#include <thread>
 
 namespace ifea {
 
@@ -46,10 +50,12 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
     //     row structures carry over node by node. Otherwise they run on the matrix itself.
     bool nodal = block > 1, sorted_rows = true;
     if (nodal) {
-        std::vector<int> nmark(nb, -1), dmark(n, -1);
+        std::vector<int> rmark(n, -1), dmark(n, -1);
         for (int b = 0; b < nb && nodal; b++) {
-            nmark[b] = b;
-            for (int p = gp[b]; p < gp[b + 1]; p++) nmark[gi[p]] = b;
+            // rows of node b's blocks: its own and its neighbours'
+            for (int c = 0; c < block; c++) rmark[b * block + c] = b;
+            for (int p = gp[b]; p < gp[b + 1]; p++)
+                for (int c = 0; c < block; c++) rmark[gi[p] * block + c] = b;
             int64_t want = (int64_t)block * (gp[b + 1] - gp[b] + 1);
             for (int c = 0; c < block && nodal; c++) {
                 int d = b * block + c;
@@ -61,7 +67,7 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
                 bool inc = true;
                 for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
                     int r = ri[p];
-                    if (r < 0 || r >= n || nmark[r / block] != b) {
+                    if ((unsigned)r >= (unsigned)n || rmark[r] != b) {
                         nodal = false;
                         break;
                     }
@@ -340,46 +346,68 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
             }
         for (int k = 0; k < m[p]; k++) pos[pb[k]] = -1;
     }
-    // original values -> fronts, grouped by level
-    a_dst.clear();
-    a_src.clear();
-    a_dst.reserve(((size_t)cp[n] + n) / 2);
-    a_src.reserve(((size_t)cp[n] + n) / 2);
-    a_level_start.assign(nlevels + 1, 0);
-    for (int l = 0; l < nlevels; l++) {
-        a_level_start[l] = (int32_t)a_src.size();
-        for (int32_t q = level_start[l]; q < level_start[l + 1]; q++) {
-            int s = level_list[q];
-            const int32_t *ib = idx.data() + idx_start[s];
-            for (int k = 0; k < m[s]; k++) pos[ib[k]] = k;
-            for (int j = c0[s]; j < c0[s] + ncol[s]; j++) {
-                int d = perm[j];
-                int64_t base = front_off[s] + (int64_t)(j - c0[s]) * m[s];
-                if (nodal && sorted_rows) {
-                    // rows come in whole node blocks, consecutive in the new numbering and in the front
-                    for (int32_t p = cp[d]; p < cp[d + 1]; p += B) {
-                        int i0 = pinv[ri[p]];
-                        if (i0 + B - 1 < j) continue;
-                        if (pos[i0] < 0) return "internal error: matrix entry outside its front";
-                        for (int r = std::max(0, j - i0); r < B; r++) {
-                            a_dst.push_back(base + pos[i0] + r);
-                            a_src.push_back(p + r);
-                        }
+    // original values -> fronts, grouped by level. The entries of one front form one range: a count pass sizes
+    // the ranges, a fill pass writes them; both hand the fronts out to host threads one at a time.
+    std::atomic<int> bad{0};
+    auto walk = [&](int q, std::vector<int32_t> &pos, int64_t *dst, int32_t *src) {
+        int s = level_list[q];
+        const int32_t *ib = idx.data() + idx_start[s];
+        for (int k = 0; k < m[s]; k++) pos[ib[k]] = k;
+        int64_t cnt = 0;
+        for (int j = c0[s]; j < c0[s] + ncol[s]; j++) {
+            int d = perm[j];
+            int64_t base = front_off[s] + (int64_t)(j - c0[s]) * m[s];
+            if (nodal && sorted_rows) {
+                // rows come in whole node blocks, consecutive in the new numbering and in the front
+                for (int32_t p = cp[d]; p < cp[d + 1]; p += B) {
+                    int i0 = pinv[ri[p]];
+                    if (i0 + B - 1 < j) continue;
+                    if (pos[i0] < 0) {
+                        bad = 1;
+                        continue;
                     }
+                    for (int r = std::max(0, j - i0); r < B; r++, cnt++)
+                        if (dst) dst[cnt] = base + pos[i0] + r, src[cnt] = p + r;
+                }
+                continue;
+            }
+            for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
+                int i = pinv[ri[p]];
+                if (i < j) continue;
+                if (pos[i] < 0) {
+                    bad = 1;
                     continue;
                 }
-                for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
-                    int i = pinv[ri[p]];
-                    if (i < j) continue;
-                    if (pos[i] < 0) return "internal error: matrix entry outside its front";
-                    a_dst.push_back(base + pos[i]);
-                    a_src.push_back(p);
-                }
+                if (dst) dst[cnt] = base + pos[i], src[cnt] = p;
+                cnt++;
             }
-            for (int k = 0; k < m[s]; k++) pos[ib[k]] = -1;
         }
-    }
-    a_level_start[nlevels] = (int32_t)a_src.size();
+        for (int k = 0; k < m[s]; k++) pos[ib[k]] = -1;
+        return cnt;
+    };
+    int nth = cp[n] < (1 << 18) ? 1 : (int)std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+    nth = std::max(1, std::min(nth, nsuper));
+    std::vector<std::vector<int32_t>> tpos(nth, std::vector<int32_t>(n, -1));
+    auto each_front = [&](const std::function<void(int, std::vector<int32_t> &)> &body) {
+        std::atomic<int> next{0};
+        auto work = [&](int t) {
+            for (int q; (q = next++) < nsuper;) body(q, tpos[t]);
+        };
+        std::vector<std::thread> th;
+        for (int t = 1; t < nth; t++) th.emplace_back(work, t);
+        work(0);
+        for (auto &x : th) x.join();
+    };
+    std::vector<int64_t> fstart(nsuper + 1, 0);  // entry range of the q-th front in level order
+    each_front([&](int q, std::vector<int32_t> &ps) { fstart[q + 1] = walk(q, ps, nullptr, nullptr); });
+    if (bad) return "internal error: matrix entry outside its front";
+    for (int q = 0; q < nsuper; q++) fstart[q + 1] += fstart[q];
+    if (fstart[nsuper] > INT32_MAX) return "Factor scatter map exceeds 32-bit indexing.";
+    a_dst.resize(fstart[nsuper]);
+    a_src.resize(fstart[nsuper]);
+    each_front([&](int q, std::vector<int32_t> &ps) { walk(q, ps, a_dst.data() + fstart[q], a_src.data() + fstart[q]); });
+    a_level_start.assign(nlevels + 1, 0);
+    for (int l = 0; l <= nlevels; l++) a_level_start[l] = (int32_t)fstart[level_start[l]];
     // extend-add schedule: r-th child (ascending) of every parent of a level
     max_rank = 1;
     for (int s = 0; s < nsuper; s++) max_rank = std::max<int>(max_rank, (int)kids[s].size());

@@ -1152,7 +1152,8 @@ public:
         d_ncol_.upload(S.ncol, st_); d_m_.upload(S.m, st_); d_c0_.upload(S.c0, st_); d_idxs_.upload(S.idx_start, st_);
         d_idx_.upload(S.idx, st_); d_rms_.upload(S.relmap_start, st_); d_rm_.upload(S.relmap, st_);
         d_uvs_.upload(S.uvec_start, st_); d_off_.upload(S.front_off, st_); d_par_.upload(S.parent, st_);
-        d_perm_.upload(S.perm, st_); d_adst_.upload(S.a_dst, st_); d_asrc_.upload(S.a_src, st_);
+        d_perm_.upload(S.perm, st_); d_adst_.upload(S.a_dst.data(), S.a_dst.size(), st_);
+        d_asrc_.upload(S.a_src.data(), S.a_src.size(), st_);
         d_ext_.upload(S.ext_child, st_);
         // children lists (ascending) for the solves
         std::vector<int32_t> cs(S.nsuper + 1, 0), cl;

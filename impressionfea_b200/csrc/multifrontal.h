@@ -6,10 +6,34 @@
 // extend-add, and the level schedule (a supernode's level = 1 + the highest level of its children).
 #pragma once
 #include <cstdint>
+#include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace ifea {
+
+// Allocator whose resize() leaves new elements uninitialised (for arrays that are written in full right after).
+template <class T>
+struct UninitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = UninitAlloc<U>;
+    };
+    UninitAlloc() = default;
+    template <class U>
+    UninitAlloc(const UninitAlloc<U> &) noexcept {}
+    template <class U>
+    void construct(U *p) noexcept
+    {
+        ::new ((void *)p) U;
+    }
+    template <class U, class... A>
+    void construct(U *p, A &&...a)
+    {
+        ::new ((void *)p) U(std::forward<A>(a)...);
+    }
+};
 
 struct MfSymbolic {
     int n = 0, nsuper = 0, nlevels = 0;
@@ -23,8 +47,8 @@ struct MfSymbolic {
     std::vector<int32_t> uvec_start;              // offset of s's update vector (nrow) in the solve pool
     int64_t uvec_pool = 0;
     // original-value scatter: dst offset in the pool <- src index into the full CSC value array
-    std::vector<int64_t> a_dst;
-    std::vector<int32_t> a_src;
+    std::vector<int64_t, UninitAlloc<int64_t>> a_dst;
+    std::vector<int32_t, UninitAlloc<int32_t>> a_src;
     std::vector<int32_t> a_level_start;           // a_dst/a_src ranges per level (fronts are stored by level)
     // level schedule
     std::vector<int32_t> level_start, level_list;  // supernodes of each level (ascending index)

@@ -17,17 +17,17 @@
 namespace {
 FILE *out = nullptr;
 
-template <class T>
-void put(const char *name, const std::vector<T> &v)
+template <class V>
+void put(const char *name, const V &v)
 {
     char nm[24] = {0};
     std::strncpy(nm, name, sizeof nm - 1);
-    int32_t eb = (int32_t)sizeof(T);
+    int32_t eb = (int32_t)sizeof(typename V::value_type);
     int64_t n = (int64_t)v.size();
     std::fwrite(nm, 1, sizeof nm, out);
     std::fwrite(&eb, 4, 1, out);
     std::fwrite(&n, 8, 1, out);
-    if (n) std::fwrite(v.data(), sizeof(T), v.size(), out);
+    if (n) std::fwrite(v.data(), eb, v.size(), out);
 }
 
 template <class T>

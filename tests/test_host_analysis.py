@@ -29,7 +29,7 @@ def driver(tmp_path_factory):
     cmd = ["g++", "-O2", "-std=c++17", "-I", CSRC, "-I", os.path.join(CUDA, "include"),
            os.path.join(ROOT, "tests", "host_analysis_driver.cpp"), os.path.join(CSRC, "mesh3d.cpp"),
            os.path.join(CSRC, "multifrontal.cpp"), "-L", os.path.join(CUDA, "lib64"), "-lcusolver",
-           "-Wl,-rpath," + os.path.join(CUDA, "lib64"), "-o", exe]
+           "-Wl,-rpath," + os.path.join(CUDA, "lib64"), "-pthread", "-o", exe]
     subprocess.check_call(cmd)
     return exe
 
