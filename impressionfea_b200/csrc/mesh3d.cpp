@@ -240,20 +240,19 @@ std::string TetTopology::build(int nn_, int ne_, const double *x, const int32_t 
     g_start.assign(nn + 1, 0);
     g_node.clear();
     gslot.assign(16 * (size_t)ne, 0);
+    std::fill(mark.begin(), mark.end(), -1);
+    std::vector<int32_t> at(nn);  // position of a node in the patch being built (valid where mark == n)
     for (int n = 0; n < nn; n++) {
-        int32_t base = (int32_t)g_node.size();
         for (int32_t q = nts[n]; q < nts[n + 1]; q++) {
             int e = ntl[q];
             for (int a = 0; a < 4; a++) {
                 int m = tets[4 * e + a];
-                int32_t idx = -1;
-                for (int32_t p = base; p < (int32_t)g_node.size(); p++)
-                    if (g_node[p] == m) { idx = p; break; }
-                if (idx < 0) {
-                    idx = (int32_t)g_node.size();
+                if (mark[m] != n) {
+                    mark[m] = n;
+                    at[m] = (int32_t)g_node.size();
                     g_node.push_back(m);
                 }
-                gslot[4 * (size_t)q + a] = idx;
+                gslot[4 * (size_t)q + a] = at[m];
             }
         }
         g_start[n + 1] = (int32_t)g_node.size();
