@@ -1080,7 +1080,6 @@ class MfSolverT final : public LinearSolver {
 public:
     explicit MfSolverT(cudaStream_t s) : st_(s)
     {
-        if (cusolverSpCreate(&hsp_) != CUSOLVER_STATUS_SUCCESS) throw Failure(IFEA_CUDA_ERROR, "cusolverSpCreate failed");
         if (cusparseCreateMatDescr(&descr_) != CUSPARSE_STATUS_SUCCESS) throw Failure(IFEA_CUDA_ERROR, "cusparseCreateMatDescr failed");
         cusparseSetMatType(descr_, CUSPARSE_MATRIX_TYPE_GENERAL);
         cusparseSetMatIndexBase(descr_, CUSPARSE_INDEX_BASE_ZERO);
@@ -1143,6 +1142,11 @@ public:
         std::string e;
         {
             HostClock hc(setup_s_[0]);
+            // the cuSOLVER handle serves the host METIS call only: made at the first analysis
+            if (!hsp_ && cusolverSpCreate(&hsp_) != CUSOLVER_STATUS_SUCCESS) {
+                hsp_ = nullptr;
+                throw Failure(IFEA_CUDA_ERROR, "cusolverSpCreate failed");
+            }
             e = sym_.analyze(n, col_ptr, row_idx, block, hsp_, descr_);
         }
         if (!e.empty()) throw Failure(IFEA_INPUT_INVALID, e);
