@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <climits>
 #include <functional>
 #include <numeric>
@@ -39,8 +40,10 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
     if (gi.empty() || !hsp) {
         std::iota(pnode.begin(), pnode.end(), 0);
     } else {
+        auto t0 = std::chrono::steady_clock::now();
         cusolverStatus_t st = cusolverSpXcsrmetisndHost((cusolverSpHandle_t)hsp, nb, (int)gi.size(), (cusparseMatDescr_t)descr,
                                                         gp.data(), gi.data(), nullptr, pnode.data());
+        order_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (st != CUSOLVER_STATUS_SUCCESS) return "METIS ordering failed (cuSOLVER status " + std::to_string((int)st) + ")";
     }
     // 1b. Steps 2-6 are structural. When every nonzero of the matrix belongs to a full block x block node block

@@ -58,6 +58,7 @@ struct MfSymbolic {
     int max_rank = 0;
     int64_t factor_nnz = 0;
     int max_m = 0, max_ncol = 0;
+    double order_s = 0;  // host seconds spent in the nested-dissection ordering (METIS) of the last analysis
 
     // Full symmetric CSC pattern (both triangles) of an n x n matrix; block = 3 orders 3x3 node blocks together.
     std::string analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block, void *cusolver_sp_handle,

@@ -750,7 +750,7 @@ struct Forging3D {
         S("t_factor", t_factor) S("t_pcg", t_pcg) S("t_final", t_final) S("t_update", t_update) S("t_total", t_total)
         S("supernodes", lin->symbolic().nsuper) S("levels", lin->symbolic().nlevels)
         S("front_pool_mb", lin->symbolic().pool * lin->value_bytes() * 1e-6) S("max_front", lin->symbolic().max_m) S("big_fronts", lin->big_fronts())
-        S("t_symbolic", lin->setup_s(0)) S("t_symbolic_dev", lin->setup_s(1)) S("t_graph_factor", lin->setup_s(2))
+        S("t_symbolic", lin->setup_s(0)) S("t_order", lin->symbolic().order_s) S("t_symbolic_dev", lin->setup_s(1)) S("t_graph_factor", lin->setup_s(2))
         S("t_graph_solve", lin->setup_s(3)) S("factor_gpu_ms", lin->factor_ms()) S("solve_gpu_ms", lin->solve_ms()) S("solves", lin->solves())
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
         S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows) S("tc_updates", lin->tc_launches())
