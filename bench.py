@@ -392,12 +392,19 @@ def run_gpu(args, rank, world):
     t0 = time.perf_counter()
     s2 = Forging3DSolver(fast_form(cfg), mesh, dies)
     s2.set_scalar("factor_fp32", 1)
+    t_setup = time.perf_counter() - t0
     d2h = 0
     for _ in range(e2e_steps):
         s2.step()
         for nm in ("x", "vg", "contact", "eps", "dmg", "el_sig", "el_rate", "el_mean"):
             d2h += s2.array(nm).nbytes
     e2e_s = time.perf_counter() - t0
+    e2e_parts = {"construct_ms": 1000.0 * t_setup}
+    for q in ("t_order", "t_symbolic", "t_symbolic_dev", "t_graph_factor", "t_graph_solve", "t_factor", "t_pcg"):
+        try:
+            e2e_parts[q[2:] + "_ms"] = 1000.0 * s2.scalar(q)
+        except Exception:
+            pass
     s2.close()
     h2d = mesh.x.nbytes + mesh.tets.nbytes + mesh.on_x0.nbytes + mesh.on_y0.nbytes + sum(d.h.nbytes for d in dies)
 
@@ -436,7 +443,8 @@ def run_gpu(args, rank, world):
                                       "achieved": a_achieved, "peak": peak, "unit": "GB/s", "frac": a_achieved / peak,
                                       "peak_kind": peak_kind, "algorithmic_bytes": abytes, "ms_per_launch": asm_ms},
                 "e2e": {"value": e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
-                        "d2h_bytes_per_step": d2h / e2e_steps},
+                        "d2h_bytes_per_step": d2h / e2e_steps, "increments": e2e_steps,
+                        "host_ms": {k: round(v, 2) for k, v in e2e_parts.items()}},
                 "gpu_launches": gpu_launches, "clocks": clocks, "closed_die": closed_die}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(budget_s=args.cpu_budget)
