@@ -5,12 +5,15 @@
 //   mesh.bin: int32 nn, ne; float64 x[3 nn]; int32 tets[4 ne]; uint8 on_x0[nn], on_y0[nn]
 //   out.bin:  records (char name[24], int32 element bytes, int64 count, data)
 // The symbolic analysis runs without a cuSOLVER handle, i.e. in the identity node order.
+//        host_analysis_driver quad <nx> <ny> <out.bin>
+//   the structured quad mesh of the 2D path (mesh2d.cpp): numbering, boundary loop and band gather maps.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
+#include "mesh2d.h"
 #include "mesh3d.h"
 #include "multifrontal.h"
 
@@ -38,8 +41,28 @@ bool get(FILE *f, std::vector<T> &v, size_t n)
 }
 }  // namespace
 
+int quad(int nx, int ny, const char *path)
+{
+    ifea::QuadTopology q;
+    std::vector<double> x;
+    std::string e = q.build_structured(nx, ny, 1.0, 0.0, 1.0, x);
+    if (!e.empty()) {
+        std::fprintf(stderr, "quad: %s\n", e.c_str());
+        return 5;
+    }
+    out = std::fopen(path, "wb");
+    if (!out) return 7;
+    std::vector<int64_t> sc = {q.nn, q.ne, q.ndof, q.half_band, q.nloop};
+    put("quad_scalars", sc), put("conn", q.conn), put("is_axis", q.is_axis), put("eq", q.eq), put("loop", q.loop);
+    put("loop_owner", q.loop_owner), put("cell_ptr", q.cell_ptr), put("cell_idx", q.cell_idx);
+    put("cell_src", q.cell_src), put("dof_ptr", q.dof_ptr), put("dof_src", q.dof_src), put("node_edge", q.node_edge);
+    std::fclose(out);
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
+    if (argc == 5 && std::strcmp(argv[1], "quad") == 0) return quad(std::atoi(argv[2]), std::atoi(argv[3]), argv[4]);
     if (argc != 4) return 2;
     FILE *f = std::fopen(argv[1], "rb");
     if (!f) return 3;

@@ -1,8 +1,10 @@
-"""Host-side analysis on the CPU: the library's topology build (mesh3d.cpp) and multifrontal symbolic analysis
-(multifrontal.cpp), compiled with g++ into a small driver (host_analysis_driver.cpp).
+"""Host-side analysis on the CPU: the library's topology builds (mesh3d.cpp, mesh2d.cpp) and multifrontal symbolic
+analysis (multifrontal.cpp), compiled with g++ into a small driver (host_analysis_driver.cpp).
 
 - The topology arrays are bit-exact with the oracle's restatement of TetMesh and BuildPattern/BuildAnp
-  (ThreeD/TetMesh.cs:18-64, Forging3DSolver.cs:469-515, :774-795, :1248-1261).
+  (ThreeD/TetMesh.cs:18-64, Forging3DSolver.cs:469-515, :774-795, :1248-1261), and the 2D quad mesh's
+  connectivity, reverse Cuthill-McKee numbering and boundary loop with the oracle's QuadMesh
+  (Mesh/QuadMesh.cs:51-221).
 - The symbolic analysis of a 3 x 3 node-block pattern runs on the node graph and expands to equations; in the
   identity order it must reproduce the equation-by-equation analysis (block 1) byte for byte, with a
   self-consistent front layout (every lower-triangle entry scattered exactly once, child rows found in the
@@ -14,9 +16,9 @@ import subprocess
 import numpy as np
 import pytest
 
-from impressionfea_b200.config import Forging3DConfig
+from impressionfea_b200.config import Forging2DConfig, Forging3DConfig
 from impressionfea_b200.meshes import gear_blank_case_3d, upset_case_3d
-from oracle import Oracle3D
+from oracle import Oracle2D, Oracle3D
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "impressionfea_b200", "csrc")
@@ -28,7 +30,7 @@ def driver(tmp_path_factory):
     exe = str(tmp_path_factory.mktemp("host") / "host_analysis_driver")
     cmd = ["g++", "-O2", "-std=c++17", "-I", CSRC, "-I", os.path.join(CUDA, "include"),
            os.path.join(ROOT, "tests", "host_analysis_driver.cpp"), os.path.join(CSRC, "mesh3d.cpp"),
-           os.path.join(CSRC, "multifrontal.cpp"), "-L", os.path.join(CUDA, "lib64"), "-lcusolver",
+           os.path.join(CSRC, "mesh2d.cpp"), os.path.join(CSRC, "multifrontal.cpp"), "-L", os.path.join(CUDA, "lib64"), "-lcusolver",
            "-Wl,-rpath," + os.path.join(CUDA, "lib64"), "-pthread", "-o", exe]
     subprocess.check_call(cmd)
     return exe
@@ -120,3 +122,21 @@ def test_front_layout_is_self_consistent(driver, tmp_path, case):
     lower = np.nonzero(pinv[ri] >= pinv[col])[0]
     assert np.array_equal(np.sort(r["a_src"]), lower)
     assert len(np.unique(r["a_dst"])) == len(r["a_dst"])
+
+
+@pytest.mark.parametrize("nx,nz", [(20, 60), (7, 5), (12, 31)])
+def test_quad_numbering_and_boundary_loop_are_bit_exact_with_the_oracle(driver, tmp_path, nx, nz):
+    op = tmp_path / "quad.bin"
+    subprocess.check_call([driver, "quad", str(nx), str(nz), str(op)])
+    got = _read(op)
+    ora = Oracle2D(Forging2DConfig(nx=nx, nz=nz))
+    try:
+        for name in ("conn", "eq", "loop", "loop_owner"):
+            np.testing.assert_array_equal(got[name], np.asarray(ora.array(name)).astype(np.int32), err_msg=name)
+        assert got["quad_scalars"][3] == ora.scalar("half_band")
+    finally:
+        ora.close()
+    # element matrix entries land in at most one band cell each; every residual entry lands in exactly one DOF
+    ne, src = nx * nz, got["cell_src"]
+    assert len(np.unique(src)) == len(src) and src.min() >= 0 and src.max() < ne * 64
+    assert np.array_equal(np.sort(got["dof_src"]), np.arange(ne * 8))
