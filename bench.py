@@ -400,7 +400,8 @@ def run_gpu(args, rank, world):
             d2h += s2.array(nm).nbytes
     e2e_s = time.perf_counter() - t0
     e2e_parts = {"construct_ms": 1000.0 * t_setup}
-    for q in ("t_order", "t_symbolic", "t_symbolic_dev", "t_graph_factor", "t_graph_solve", "t_factor", "t_pcg"):
+    for q in ("t_order", "t_symbolic", "t_symbolic_wait", "t_symbolic_dev", "t_graph_factor", "t_graph_solve",
+              "t_factor", "t_pcg"):
         try:
             e2e_parts[q[2:] + "_ms"] = 1000.0 * s2.scalar(q)
         except Exception:

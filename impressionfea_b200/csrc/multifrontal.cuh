@@ -1047,6 +1047,7 @@ public:
     virtual ~LinearSolver() = default;
     virtual void set_stream(cudaStream_t s) = 0;
     virtual void analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block) = 0;
+    virtual void analyze_from(MfSymbolic &&S) = 0;  // the same, from a symbolic analysis made elsewhere
     virtual void factorize(const double *d_full_vals) = 0;
     virtual void solve(const double *d_b, double *d_x) = 0;
     virtual void check_finite(const double *d_x) = 0;
@@ -1150,6 +1151,20 @@ public:
             e = sym_.analyze(n, col_ptr, row_idx, block, hsp_, descr_);
         }
         if (!e.empty()) throw Failure(IFEA_INPUT_INVALID, e);
+        device_tables();
+    }
+
+    void analyze_from(MfSymbolic &&S) override
+    {
+        analyzed_ = factored_ = false;
+        drop_graphs();
+        sym_ = std::move(S);
+        device_tables();
+    }
+
+    // Device copies of the symbolic analysis, solve schedules, pivot-block inverse tasks and kernel attributes.
+    void device_tables()
+    {
         HostClock hc(setup_s_[1]);
         const MfSymbolic &S = sym_;
 
@@ -1307,7 +1322,7 @@ public:
         small_smem_ = (size_t)max_small_m * sizeof(T);
         d_F_.resize(S.pool);
         d_U_.resize(std::max<int64_t>(S.uvec_pool, 1));
-        d_y_.resize(n);
+        d_y_.resize(S.n);
         dev_.ncol = d_ncol_; dev_.m = d_m_; dev_.c0 = d_c0_; dev_.idx_start = d_idxs_; dev_.idx = d_idx_;
         dev_.relmap_start = d_rms_; dev_.relmap = d_rm_; dev_.uvec_start = d_uvs_; dev_.child_start = d_cs_;
         dev_.child_list = d_cl_; dev_.front_off = d_off_; dev_.F = d_F_; dev_.U = d_U_;

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -57,6 +58,12 @@ struct Forging3D {
     double load = 0, reaction = 0, power = 0, last_dt = 0, rnorm = 0, beta_last = 0, max_diag = 0;
     // linear solver (SolveLinear :965-1019)
     std::unique_ptr<LinearSolver> lin;
+    // symbolic analysis of the pattern (METIS ordering included), started on a host thread when the mesh is set
+    // and taken by the first factorisation; the job reads only topo's pattern, which nothing writes meanwhile
+    std::thread sym_job;
+    std::unique_ptr<MfSymbolic> sym_pre;
+    std::string sym_err;
+    double t_sym_wait = 0;
     bool need_analyze = true, have_factor = false;
     // single-precision factor refined by FP64 PCG (off: the reference's FP64 direct solve after a factorisation)
     bool factor_fp32 = false;
@@ -109,6 +116,7 @@ struct Forging3D {
     bool own_stream = true;
     ~Forging3D()
     {
+        join_analysis();
         if (st) cudaStreamSynchronize(st);
         lin.reset();
         if (st && own_stream) cudaStreamDestroy(st);
@@ -194,10 +202,77 @@ struct Forging3D {
     }
 
     // ---------------------------------------------------------------- setup
+    void join_analysis()
+    {
+        if (sym_job.joinable()) sym_job.join();
+    }
+
+    void start_analysis()
+    {
+        join_analysis();
+        sym_pre.reset();
+        sym_err.clear();
+        int dev = 0;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        sym_job = std::thread([this, dev] {
+            cusolverSpHandle_t hsp = nullptr;
+            cusparseMatDescr_t descr = nullptr;
+            try {
+                cudaSetDevice(dev);
+                if (cusolverSpCreate(&hsp) != CUSOLVER_STATUS_SUCCESS) {
+                    hsp = nullptr;
+                    sym_err = "cusolverSpCreate failed";
+                } else if (cusparseCreateMatDescr(&descr) != CUSPARSE_STATUS_SUCCESS) {
+                    descr = nullptr;
+                    sym_err = "cusparseCreateMatDescr failed";
+                } else {
+                    cusparseSetMatType(descr, CUSPARSE_MATRIX_TYPE_GENERAL);
+                    cusparseSetMatIndexBase(descr, CUSPARSE_INDEX_BASE_ZERO);
+                    std::unique_ptr<MfSymbolic> S(new MfSymbolic);
+                    std::string e = S->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3, hsp, descr);
+                    if (e.empty())
+                        sym_pre = std::move(S);
+                    else
+                        sym_err = e;
+                }
+            } catch (std::exception &x) {
+                sym_err = x.what();
+            } catch (...) {
+                sym_err = "symbolic analysis failed";
+            }
+            if (descr) cusparseDestroyMatDescr(descr);
+            if (hsp) cusolverSpDestroy(hsp);
+        });
+    }
+
+    // the analysis for the next factorisation: the one started with the mesh when it is there, else made now
+    void analyze_pattern()
+    {
+        if (sym_job.joinable() || sym_pre || !sym_err.empty()) {
+            {
+                PhaseTimer pt(t_sym_wait);
+                join_analysis();
+            }
+            if (!sym_pre) {
+                std::string e = sym_err.empty() ? "symbolic analysis failed" : sym_err;
+                sym_err.clear();
+                throw Failure(IFEA_INPUT_INVALID, e);
+            }
+            lin->analyze_from(std::move(*sym_pre));
+            sym_pre.reset();
+        } else {
+            lin->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3);
+        }
+    }
+
     void set_mesh(int nn, int ne, const double *x, const int32_t *tets, const uint8_t *ox, const uint8_t *oy)
     {
+        join_analysis();
+        sym_pre.reset();
+        sym_err.clear();
         std::string e = topo.build(nn, ne, x, tets, ox, oy);
         if (!e.empty()) throw Failure(IFEA_INPUT_INVALID, e);
+        start_analysis();
         std::vector<double> hl = local_lengths(topo, x, h);
         d_tets.upload(topo.tets, st); d_nts.upload(topo.nts, st); d_ntl.upload(topo.ntl, st); d_qk.upload(topo.qk, st);
         d_gslot.upload(topo.gslot, st); d_bface.upload(topo.bface, st); d_bowner.upload(topo.bowner, st);
@@ -435,7 +510,7 @@ struct Forging3D {
             if (++pcg_failures >= 2) pcg_skip = std::min(64, 1 << (pcg_failures - 1));
         }
         if (need_analyze) {
-            lin->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3);
+            analyze_pattern();
             need_analyze = false;
         }
         try {
@@ -750,7 +825,7 @@ struct Forging3D {
         S("t_factor", t_factor) S("t_pcg", t_pcg) S("t_final", t_final) S("t_update", t_update) S("t_total", t_total)
         S("supernodes", lin->symbolic().nsuper) S("levels", lin->symbolic().nlevels)
         S("front_pool_mb", lin->symbolic().pool * lin->value_bytes() * 1e-6) S("max_front", lin->symbolic().max_m) S("big_fronts", lin->big_fronts())
-        S("t_symbolic", lin->setup_s(0)) S("t_order", lin->symbolic().order_s) S("t_symbolic_dev", lin->setup_s(1)) S("t_graph_factor", lin->setup_s(2))
+        S("t_symbolic", lin->setup_s(0)) S("t_order", lin->symbolic().order_s) S("t_symbolic_wait", t_sym_wait) S("t_symbolic_dev", lin->setup_s(1)) S("t_graph_factor", lin->setup_s(2))
         S("t_graph_solve", lin->setup_s(3)) S("factor_gpu_ms", lin->factor_ms()) S("solve_gpu_ms", lin->solve_ms()) S("solves", lin->solves())
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
         S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows) S("tc_updates", lin->tc_launches())
