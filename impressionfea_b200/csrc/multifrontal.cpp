@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <chrono>
 #include <climits>
 #include <functional>
@@ -14,7 +15,128 @@
 
 namespace ifea {
 
-std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, int block, void *hsp, void *descr)
+namespace {
+// Nested dissection by coordinate cuts: a set of more than kLeaf nodes is split by a plane normal to one axis at
+// 40-60 % of its nodes, choosing among the three axes and five positions the cut whose smaller one-sided
+// boundary (the nodes on one side with a neighbour on the other) is smallest, with a penalty for imbalance.
+// That boundary is the separator, numbered after both halves; halves recurse, leaves keep ascending node order.
+// A node can only neighbour the other side from within reach[ax] of the plane (its longest edge along that axis),
+// so each candidate cut scans a slab, not the set. Every list is kept in ascending node order between steps.
+struct CoordNd {
+    static constexpr int kLeaf = 32;
+    int nb;
+    const int *gp, *gi;
+    const double *x;
+    std::vector<int32_t> mark, perm_rev;  // perm_rev: nodes in reverse elimination order
+    std::vector<double> reach[3];
+    int stamp = 0;
+
+    double X(int v, int ax) const { return x[3 * (size_t)v + ax]; }
+    bool less(int a, int b, int ax) const { return X(a, ax) < X(b, ax) || (X(a, ax) == X(b, ax) && a < b); }
+
+    void run(int32_t *pnode)
+    {
+        mark.assign(nb, 0);
+        for (int ax = 0; ax < 3; ax++) {
+            reach[ax].assign(nb, 0.0);
+            for (int v = 0; v < nb; v++)
+                for (int p = gp[v]; p < gp[v + 1]; p++) reach[ax][v] = std::max(reach[ax][v], std::fabs(X(v, ax) - X(gi[p], ax)));
+        }
+        std::vector<int> all(nb);
+        std::iota(all.begin(), all.end(), 0);
+        perm_rev.clear();
+        split(all);
+        for (int k = 0; k < nb; k++) pnode[k] = perm_rev[nb - 1 - k];
+    }
+
+    // one-sided boundary of side A of the cut arr[0, mid) | arr[mid, n) (A = left when left is true)
+    void boundary(const std::vector<int> &arr, int mid, int ax, double mr, bool left, int in_set, std::vector<int> &out)
+    {
+        out.clear();
+        int n = (int)arr.size(), piv = arr[mid], last = arr[mid - 1];
+        if (left) {
+            for (int i = mid - 1; i >= 0 && X(arr[i], ax) >= X(piv, ax) - mr; i--) {
+                int v = arr[i];
+                for (int p = gp[v]; p < gp[v + 1]; p++) {
+                    int w = gi[p];
+                    if (mark[w] == in_set && !less(w, piv, ax)) {
+                        out.push_back(v);
+                        break;
+                    }
+                }
+            }
+        } else {
+            for (int i = mid; i < n && X(arr[i], ax) <= X(last, ax) + mr; i++) {
+                int v = arr[i];
+                for (int p = gp[v]; p < gp[v + 1]; p++) {
+                    int w = gi[p];
+                    if (mark[w] == in_set && less(w, piv, ax)) {
+                        out.push_back(v);
+                        break;
+                    }
+                }
+            }
+        }
+    }
+
+    void split(std::vector<int> &set)  // set: ascending node ids
+    {
+        int n = (int)set.size();
+        if (n <= kLeaf) {
+            for (int i = n - 1; i >= 0; i--) perm_rev.push_back(set[i]);
+            return;
+        }
+        int in_set = ++stamp;
+        for (int v : set) mark[v] = in_set;
+        double best = 1e300;
+        int best_ax = -1, best_mid = 0;
+        bool best_left = true;
+        std::vector<int> arr[3], bnd;
+        for (int ax = 0; ax < 3; ax++) {
+            arr[ax] = set;
+            std::sort(arr[ax].begin(), arr[ax].end(), [&](int a, int b) { return less(a, b, ax); });
+            double mr = 0;
+            for (int v : set) mr = std::max(mr, reach[ax][v]);
+            for (int f = 40; f <= 60; f += 5) {
+                int mid = (int)((int64_t)n * f / 100);
+                if (mid < 1 || mid >= n) continue;
+                for (int side = 0; side < 2; side++) {
+                    boundary(arr[ax], mid, ax, mr, side == 0, in_set, bnd);
+                    double s = (double)bnd.size();
+                    double big = side == 0 ? std::max(mid - s, (double)(n - mid)) : std::max((double)mid, n - mid - s);
+                    double cost = s * (1.0 + 2.0 * std::max(0.0, big / n - 0.5));
+                    if (cost < best) {
+                        best = cost, best_ax = ax, best_mid = mid, best_left = side == 0;
+                    }
+                }
+            }
+        }
+        boundary(arr[best_ax], best_mid, best_ax, [&] {
+            double mr = 0;
+            for (int v : set) mr = std::max(mr, reach[best_ax][v]);
+            return mr;
+        }(), best_left, in_set, bnd);
+        int in_sep = ++stamp;
+        for (int v : bnd) mark[v] = in_sep;
+        std::vector<int> L, R;
+        const std::vector<int> &a = arr[best_ax];
+        for (int i = 0; i < n; i++)
+            if (mark[a[i]] != in_sep) (i < best_mid ? L : R).push_back(a[i]);
+        std::sort(bnd.begin(), bnd.end());
+        std::sort(L.begin(), L.end());
+        std::sort(R.begin(), R.end());
+        for (int i = (int)bnd.size() - 1; i >= 0; i--) perm_rev.push_back(bnd[i]);
+        std::vector<int>().swap(arr[0]), std::vector<int>().swap(arr[1]), std::vector<int>().swap(arr[2]);
+        set.clear();
+        set.shrink_to_fit();
+        split(R);
+        split(L);
+    }
+};
+}  // namespace
+
+std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, int block, void *hsp, void *descr,
+                                const double *node_xyz)
 {
     n = n_;
     if (n <= 0) return "empty system";
@@ -37,7 +159,12 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
         }
     }
     std::vector<int> pnode(nb);
-    if (gi.empty() || !hsp) {
+    if (!gi.empty() && node_xyz) {
+        auto t0 = std::chrono::steady_clock::now();
+        CoordNd nd{nb, gp.data(), gi.data(), node_xyz};
+        nd.run(pnode.data());
+        order_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    } else if (gi.empty() || !hsp) {
         std::iota(pnode.begin(), pnode.end(), 0);
     } else {
         auto t0 = std::chrono::steady_clock::now();

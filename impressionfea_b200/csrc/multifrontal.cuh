@@ -1046,7 +1046,9 @@ class LinearSolver {
 public:
     virtual ~LinearSolver() = default;
     virtual void set_stream(cudaStream_t s) = 0;
-    virtual void analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block) = 0;
+    // node_xyz (3 coordinates per node): coordinate nested dissection instead of METIS
+    virtual void analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block,
+                         const double *node_xyz = nullptr) = 0;
     virtual void analyze_from(MfSymbolic &&S) = 0;  // the same, from a symbolic analysis made elsewhere
     virtual void factorize(const double *d_full_vals) = 0;
     virtual void solve(const double *d_b, double *d_x) = 0;
@@ -1136,19 +1138,19 @@ public:
     void set_wide_rows(int m) override { wide_m_ = m; }
     int n() const { return sym_.n; }
 
-    void analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block) override
+    void analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block, const double *node_xyz = nullptr) override
     {
         analyzed_ = factored_ = false;
         drop_graphs();
         std::string e;
         {
             HostClock hc(setup_s_[0]);
-            // the cuSOLVER handle serves the host METIS call only: made at the first analysis
-            if (!hsp_ && cusolverSpCreate(&hsp_) != CUSOLVER_STATUS_SUCCESS) {
+            // the cuSOLVER handle serves the host METIS call only: made at the first analysis that orders by METIS
+            if (!node_xyz && !hsp_ && cusolverSpCreate(&hsp_) != CUSOLVER_STATUS_SUCCESS) {
                 hsp_ = nullptr;
                 throw Failure(IFEA_CUDA_ERROR, "cusolverSpCreate failed");
             }
-            e = sym_.analyze(n, col_ptr, row_idx, block, hsp_, descr_);
+            e = sym_.analyze(n, col_ptr, row_idx, block, hsp_, descr_, node_xyz);
         }
         if (!e.empty()) throw Failure(IFEA_INPUT_INVALID, e);
         device_tables();

@@ -61,8 +61,10 @@ struct MfSymbolic {
     double order_s = 0;  // host seconds spent in the nested-dissection ordering (METIS) of the last analysis
 
     // Full symmetric CSC pattern (both triangles) of an n x n matrix; block = 3 orders 3x3 node blocks together.
+    // The node order is METIS nested dissection through cuSOLVER's host helper, or, when node_xyz (3 coordinates
+    // per node) is given, this file's coordinate nested dissection (coordinate_nd).
     std::string analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block, void *cusolver_sp_handle,
-                        void *mat_descr);
+                        void *mat_descr, const double *node_xyz = nullptr);
 };
 
 }  // namespace ifea

@@ -58,12 +58,16 @@ struct Forging3D {
     double load = 0, reaction = 0, power = 0, last_dt = 0, rnorm = 0, beta_last = 0, max_diag = 0;
     // linear solver (SolveLinear :965-1019)
     std::unique_ptr<LinearSolver> lin;
-    // symbolic analysis of the pattern (METIS ordering included), started on a host thread when the mesh is set
-    // and taken by the first factorisation; the job reads only topo's pattern, which nothing writes meanwhile
+    // Symbolic analysis of the pattern, started on a host thread when the mesh is set and taken by the first
+    // factorisation; the job reads only topo's pattern and node_xyz, which nothing writes meanwhile. Node order
+    // (`ordering`): 0 (default) METIS; 1 coordinate nested dissection (13 ms instead of 86 ms to compute on the
+    // 31.9k-tet case, about 7 % slower factorisations: a longer panel chain).
     std::thread sym_job;
     std::unique_ptr<MfSymbolic> sym_pre;
     std::string sym_err;
     double t_sym_wait = 0;
+    int ordering = 0;
+    std::vector<double> node_xyz;  // node coordinates when the mesh was set
     bool need_analyze = true, have_factor = false;
     // single-precision factor refined by FP64 PCG (off: the reference's FP64 direct solve after a factorisation)
     bool factor_fp32 = false;
@@ -207,6 +211,38 @@ struct Forging3D {
         if (sym_job.joinable()) sym_job.join();
     }
 
+    // one analysis on the calling (job) thread: coordinate order when xyz is given, else METIS
+    void analysis_job(int dev, const double *xyz, std::unique_ptr<MfSymbolic> *out, std::string *err)
+    {
+        cusolverSpHandle_t hsp = nullptr;
+        cusparseMatDescr_t descr = nullptr;
+        try {
+            cudaSetDevice(dev);
+            if (!xyz && cusolverSpCreate(&hsp) != CUSOLVER_STATUS_SUCCESS) {
+                hsp = nullptr;
+                *err = "cusolverSpCreate failed";
+            } else if (cusparseCreateMatDescr(&descr) != CUSPARSE_STATUS_SUCCESS) {
+                descr = nullptr;
+                *err = "cusparseCreateMatDescr failed";
+            } else {
+                cusparseSetMatType(descr, CUSPARSE_MATRIX_TYPE_GENERAL);
+                cusparseSetMatIndexBase(descr, CUSPARSE_INDEX_BASE_ZERO);
+                std::unique_ptr<MfSymbolic> S(new MfSymbolic);
+                std::string e = S->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3, hsp, descr, xyz);
+                if (e.empty())
+                    *out = std::move(S);
+                else
+                    *err = e;
+            }
+        } catch (std::exception &x) {
+            *err = x.what();
+        } catch (...) {
+            *err = "symbolic analysis failed";
+        }
+        if (descr) cusparseDestroyMatDescr(descr);
+        if (hsp) cusolverSpDestroy(hsp);
+    }
+
     void start_analysis()
     {
         join_analysis();
@@ -214,35 +250,8 @@ struct Forging3D {
         sym_err.clear();
         int dev = 0;
         cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-        sym_job = std::thread([this, dev] {
-            cusolverSpHandle_t hsp = nullptr;
-            cusparseMatDescr_t descr = nullptr;
-            try {
-                cudaSetDevice(dev);
-                if (cusolverSpCreate(&hsp) != CUSOLVER_STATUS_SUCCESS) {
-                    hsp = nullptr;
-                    sym_err = "cusolverSpCreate failed";
-                } else if (cusparseCreateMatDescr(&descr) != CUSPARSE_STATUS_SUCCESS) {
-                    descr = nullptr;
-                    sym_err = "cusparseCreateMatDescr failed";
-                } else {
-                    cusparseSetMatType(descr, CUSPARSE_MATRIX_TYPE_GENERAL);
-                    cusparseSetMatIndexBase(descr, CUSPARSE_INDEX_BASE_ZERO);
-                    std::unique_ptr<MfSymbolic> S(new MfSymbolic);
-                    std::string e = S->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3, hsp, descr);
-                    if (e.empty())
-                        sym_pre = std::move(S);
-                    else
-                        sym_err = e;
-                }
-            } catch (std::exception &x) {
-                sym_err = x.what();
-            } catch (...) {
-                sym_err = "symbolic analysis failed";
-            }
-            if (descr) cusparseDestroyMatDescr(descr);
-            if (hsp) cusolverSpDestroy(hsp);
-        });
+        const double *xyz = ordering == 1 ? node_xyz.data() : nullptr;
+        sym_job = std::thread([this, dev, xyz] { analysis_job(dev, xyz, &sym_pre, &sym_err); });
     }
 
     // the analysis for the next factorisation: the one started with the mesh when it is there, else made now
@@ -261,7 +270,7 @@ struct Forging3D {
             lin->analyze_from(std::move(*sym_pre));
             sym_pre.reset();
         } else {
-            lin->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3);
+            lin->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3, ordering == 1 ? node_xyz.data() : nullptr);
         }
     }
 
@@ -272,6 +281,7 @@ struct Forging3D {
         sym_err.clear();
         std::string e = topo.build(nn, ne, x, tets, ox, oy);
         if (!e.empty()) throw Failure(IFEA_INPUT_INVALID, e);
+        node_xyz.assign(x, x + 3 * (size_t)nn);
         start_analysis();
         std::vector<double> hl = local_lengths(topo, x, h);
         d_tets.upload(topo.tets, st); d_nts.upload(topo.nts, st); d_ntl.upload(topo.ntl, st); d_qk.upload(topo.qk, st);
@@ -522,7 +532,8 @@ struct Forging3D {
                 if (f.status != IFEA_NOT_SPD || lin->value_bytes() == 8) throw;
                 use_precision(false);
                 fp32_fallbacks++;
-                lin->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3);
+                lin->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3,
+                             ordering == 1 ? node_xyz.data() : nullptr);
                 need_analyze = false;
                 lin->factorize(d_val);
             }
@@ -825,7 +836,7 @@ struct Forging3D {
         S("t_factor", t_factor) S("t_pcg", t_pcg) S("t_final", t_final) S("t_update", t_update) S("t_total", t_total)
         S("supernodes", lin->symbolic().nsuper) S("levels", lin->symbolic().nlevels)
         S("front_pool_mb", lin->symbolic().pool * lin->value_bytes() * 1e-6) S("max_front", lin->symbolic().max_m) S("big_fronts", lin->big_fronts())
-        S("t_symbolic", lin->setup_s(0)) S("t_order", lin->symbolic().order_s) S("t_symbolic_wait", t_sym_wait) S("t_symbolic_dev", lin->setup_s(1)) S("t_graph_factor", lin->setup_s(2))
+        S("ordering", ordering) S("t_symbolic", lin->setup_s(0)) S("t_order", lin->symbolic().order_s) S("t_symbolic_wait", t_sym_wait) S("t_symbolic_dev", lin->setup_s(1)) S("t_graph_factor", lin->setup_s(2))
         S("t_graph_solve", lin->setup_s(3)) S("factor_gpu_ms", lin->factor_ms()) S("solve_gpu_ms", lin->solve_ms()) S("solves", lin->solves())
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
         S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows) S("tc_updates", lin->tc_launches())
@@ -852,6 +863,15 @@ struct Forging3D {
             use_precision(v != 0);
             pcg_early_abort = v != 0;
         } else if (nm == "pcg_early_abort") pcg_early_abort = v != 0;
+        else if (nm == "ordering") {
+            if (v != 0 && v != 1) throw Failure(IFEA_INPUT_INVALID, "ordering: 0 (METIS) or 1 (coordinate nested dissection)");
+            if ((int)v != ordering) {
+                ordering = (int)v;
+                if (topo.nn > 0) start_analysis();
+                need_analyze = true;
+                have_factor = false;
+            }
+        }
         else throw Failure(IFEA_INPUT_INVALID, "unknown scalar name '" + nm + "'");
     }
 };

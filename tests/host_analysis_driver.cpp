@@ -1,10 +1,11 @@
 // Host-side analysis driver for the CPU tests: builds the library's tetrahedral topology (mesh3d.cpp) and the
 // multifrontal symbolic analysis (multifrontal.cpp) from a mesh file and writes every array they produce.
 //
-// usage: host_analysis_driver <mesh.bin> <out.bin> <block>
+// usage: host_analysis_driver <mesh.bin> <out.bin> <block> [xyz]
 //   mesh.bin: int32 nn, ne; float64 x[3 nn]; int32 tets[4 ne]; uint8 on_x0[nn], on_y0[nn]
 //   out.bin:  records (char name[24], int32 element bytes, int64 count, data)
-// The symbolic analysis runs without a cuSOLVER handle, i.e. in the identity node order.
+// The symbolic analysis runs without a cuSOLVER handle, i.e. in the identity node order, or with "xyz" in the
+// coordinate nested-dissection order.
 //        host_analysis_driver quad <nx> <ny> <out.bin>
 //   the structured quad mesh of the 2D path (mesh2d.cpp): numbering, boundary loop and band gather maps.
 #include <cstdio>
@@ -63,7 +64,8 @@ int quad(int nx, int ny, const char *path)
 int main(int argc, char **argv)
 {
     if (argc == 5 && std::strcmp(argv[1], "quad") == 0) return quad(std::atoi(argv[2]), std::atoi(argv[3]), argv[4]);
-    if (argc != 4) return 2;
+    if (argc != 4 && argc != 5) return 2;
+    bool xyz = argc == 5 && std::strcmp(argv[4], "xyz") == 0;
     FILE *f = std::fopen(argv[1], "rb");
     if (!f) return 3;
     int32_t hdr[2];
@@ -82,7 +84,8 @@ int main(int argc, char **argv)
         return 5;
     }
     ifea::MfSymbolic S;
-    e = S.analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), std::atoi(argv[3]), nullptr, nullptr);
+    e = S.analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), std::atoi(argv[3]), nullptr, nullptr,
+                  xyz ? x.data() : nullptr);
     if (!e.empty()) {
         std::fprintf(stderr, "symbolic: %s\n", e.c_str());
         return 6;

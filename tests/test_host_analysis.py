@@ -49,15 +49,15 @@ def _read(path):
             out[name.rstrip(b"\0").decode()] = np.frombuffer(f.read(eb * n), dt[eb]).copy()
 
 
-def _run(driver, tmp_path, mesh, block):
-    mp, op = tmp_path / "mesh.bin", tmp_path / f"out{block}.bin"
+def _run(driver, tmp_path, mesh, block, order=None):
+    mp, op = tmp_path / "mesh.bin", tmp_path / f"out{block}{order or ''}.bin"
     with open(mp, "wb") as f:
         np.array([len(mesh.x), len(mesh.tets)], np.int32).tofile(f)
         np.ascontiguousarray(mesh.x, np.float64).tofile(f)
         np.ascontiguousarray(mesh.tets, np.int32).tofile(f)
         np.ascontiguousarray(mesh.on_x0, np.uint8).tofile(f)
         np.ascontiguousarray(mesh.on_y0, np.uint8).tofile(f)
-    subprocess.check_call([driver, str(mp), str(op), str(block)])
+    subprocess.check_call([driver, str(mp), str(op), str(block)] + ([order] if order else []))
     return _read(op)
 
 
@@ -100,9 +100,10 @@ def test_nodal_symbolic_analysis_matches_equation_level(driver, tmp_path, case):
         np.testing.assert_array_equal(nodal[name], eqn[name], err_msg=name)
 
 
+@pytest.mark.parametrize("order", [None, "xyz"])
 @pytest.mark.parametrize("case", sorted(CASES))
-def test_front_layout_is_self_consistent(driver, tmp_path, case):
-    r = _run(driver, tmp_path, CASES[case][0], 3)
+def test_front_layout_is_self_consistent(driver, tmp_path, case, order):
+    r = _run(driver, tmp_path, CASES[case][0], 3, order)
     n, nsuper = int(r["sym_scalars"][0]), int(r["sym_scalars"][1])
     perm, pinv, cp, ri = r["perm"], r["pinv"], r["col_ptr"], r["row_idx"]
     assert np.array_equal(np.sort(perm), np.arange(n)) and np.array_equal(pinv[perm], np.arange(n))
@@ -140,3 +141,16 @@ def test_quad_numbering_and_boundary_loop_are_bit_exact_with_the_oracle(driver, 
     ne, src = nx * nz, got["cell_src"]
     assert len(np.unique(src)) == len(src) and src.min() >= 0 and src.max() < ne * 64
     assert np.array_equal(np.sort(got["dof_src"]), np.arange(ne * 8))
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_coordinate_dissection_separates_its_halves(driver, tmp_path, case):
+    """Coordinate nested dissection: the order is a permutation of whole node blocks and every supernode's parent is
+    eliminated after it (the front layout itself is checked by test_front_layout_is_self_consistent)."""
+    r = _run(driver, tmp_path, CASES[case][0], 3, "xyz")
+    perm, n = r["perm"], int(r["sym_scalars"][0])
+    assert np.array_equal(np.sort(perm), np.arange(n))
+    assert np.array_equal(perm.reshape(-1, 3) % 3, np.tile(np.arange(3), (n // 3, 1)))
+    assert np.all(perm.reshape(-1, 3)[:, 1] == perm.reshape(-1, 3)[:, 0] + 1)
+    parent = r["parent"]
+    assert np.all((parent == -1) | (parent > np.arange(len(parent))))
