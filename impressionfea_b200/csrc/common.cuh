@@ -150,24 +150,6 @@ IFEA_HD double principal_max3(double xx, double yy, double zz, double xy, double
     return q + 2 * p * cos(phi);
 }
 
-// Order-preserving encoding of doubles for atomicMax/atomicMin on 64-bit integers.
-__device__ __forceinline__ long long dbl_order_key(double v)
-{
-    long long b = __double_as_longlong(v);
-    return b >= 0 ? b : (b ^ 0x7fffffffffffffffLL);
-}
-__host__ __device__ __forceinline__ double dbl_from_key(long long k)
-{
-    long long b = k >= 0 ? k : (k ^ 0x7fffffffffffffffLL);
-#ifdef __CUDA_ARCH__
-    return __longlong_as_double(b);
-#else
-    double d;
-    memcpy(&d, &b, 8);
-    return d;
-#endif
-}
-
 #define IFEA_CUDA_CHECK(call)                                                                                   \
     do {                                                                                                        \
         cudaError_t _e = (call);                                                                                \

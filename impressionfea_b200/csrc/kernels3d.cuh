@@ -568,15 +568,6 @@ __global__ void k_regularise(View3 V)
     }
 }
 
-// r := 0 on fixed DOFs (after the fused assembly the residual still holds the raw values)
-__global__ void k_zero_fixed_r(View3 V)
-{
-    GRID_STRIDE(d, V.ndof)
-    {
-        if (V.fixed[d]) V.r[d] = 0.0;
-    }
-}
-
 // y = A x with A the assembled values in 3x3 node blocks, row form: one warp per node.
 __global__ void k_spmv(View3 V, const double *__restrict__ x, double *__restrict__ y)
 {
@@ -749,11 +740,6 @@ __global__ void k_predict(View3 V, double dt, double gapT, double tol_h, int len
     }
     const int s[1] = {S_MAXPEN};
     emit_max<1>(V, mx, s);
-}
-
-__global__ void k_quality(View3 V, const double *x, double *q)
-{
-    GRID_STRIDE(e, V.ne) { q[e] = quality_of(V, x, e); }
 }
 
 // min quality (as a max of -q) and the lowest element index with q <= thr (err[1])
