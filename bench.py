@@ -264,6 +264,19 @@ def _count_launches(cfg, mesh, dies, stream, warmup, k, fp32):
         return None
 
 
+def whole_job_value(total_ms, k, world, device="cuda"):
+    """Increments per second of the whole job: every rank ran k increments and the job took as long as its
+    slowest rank (max over ranks of each rank's device time). Returns (value, that time in ms)."""
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    return world * k / (total_ms / 1000.0), total_ms
+
+
 def run_gpu(args, rank, world):
     import torch
 
@@ -303,13 +316,7 @@ def run_gpu(args, rank, world):
         durs, infos, snaps = _timed_steps(s, stream, flush, args.steps, snap)
     torch.cuda.synchronize()
     k = len(durs)
-    total_ms = float(sum(durs))
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-        torch.distributed.barrier()
-    value = world * k / (total_ms / 1000.0)
+    value, total_ms = whole_job_value(float(sum(durs)), k, world)
     ms64 = float(sum(durs64)) / len(durs64) if durs64 else None
 
     # a tightly converged FP64 reference (Newton tolerance 1e-6) over the same increments, untimed: the plain
