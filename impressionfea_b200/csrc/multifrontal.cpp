@@ -16,18 +16,20 @@
 namespace ifea {
 
 namespace {
-// Nested dissection by coordinate cuts: a set of more than kLeaf nodes is split by a plane normal to one axis at
-// 40-60 % of its nodes, choosing among the three axes and five positions the cut whose smaller one-sided
-// boundary (the nodes on one side with a neighbour on the other) is smallest, with a penalty for imbalance.
-// That boundary is the separator, numbered after both halves; halves recurse, leaves keep ascending node order.
-// A node can only neighbour the other side from within reach[ax] of the plane (its longest edge along that axis),
-// so each candidate cut scans a slab, not the set. Every list is kept in ascending node order between steps.
+// Nested dissection by coordinate cuts. A set of more than kLeaf nodes is cut by a plane normal to one axis at
+// 40-60 % of its nodes; among the three axes and five positions the cut whose smaller one-sided boundary (the
+// nodes of one side with a neighbour on the other) is smallest, with a penalty for imbalance, wins, and that
+// boundary is the separator. On the kCoverDepth top levels the separator is then reduced to a minimum vertex
+// cover of the edges across the cut (maximum bipartite matching and König's theorem) when that is smaller. The
+// separator is numbered after both halves, which recurse; leaves keep their order. A node can only neighbour the
+// other side from within reach[ax] of the plane (its longest edge along that axis), so the boundary scans cover a
+// slab of the sorted set, not all of it.
 struct CoordNd {
-    static constexpr int kLeaf = 32;
+    static constexpr int kLeaf = 32, kCoverDepth = 2;
     int nb;
     const int *gp, *gi;
     const double *x;
-    std::vector<int32_t> mark, perm_rev;  // perm_rev: nodes in reverse elimination order
+    std::vector<int32_t> mark, perm_rev, loc, vis;  // perm_rev: nodes in reverse elimination order
     std::vector<double> reach[3];
     int stamp = 0;
 
@@ -37,6 +39,7 @@ struct CoordNd {
     void run(int32_t *pnode)
     {
         mark.assign(nb, 0);
+        loc.assign(nb, -1);
         for (int ax = 0; ax < 3; ax++) {
             reach[ax].assign(nb, 0.0);
             for (int v = 0; v < nb; v++)
@@ -45,41 +48,130 @@ struct CoordNd {
         std::vector<int> all(nb);
         std::iota(all.begin(), all.end(), 0);
         perm_rev.clear();
-        split(all);
+        split(all, 0);
         for (int k = 0; k < nb; k++) pnode[k] = perm_rev[nb - 1 - k];
     }
 
-    // one-sided boundary of side A of the cut arr[0, mid) | arr[mid, n) (A = left when left is true)
-    void boundary(const std::vector<int> &arr, int mid, int ax, double mr, bool left, int in_set, std::vector<int> &out)
+    // one-sided boundary of the cut arr[0, mid) | arr[mid, n), in arr order; stops once it holds `limit` nodes
+    void boundary(const std::vector<int> &arr, int mid, int ax, double mr, bool left, int in_set, std::vector<int> &out,
+                  size_t limit)
     {
         out.clear();
         int n = (int)arr.size(), piv = arr[mid], last = arr[mid - 1];
         if (left) {
-            for (int i = mid - 1; i >= 0 && X(arr[i], ax) >= X(piv, ax) - mr; i--) {
+            double lo = X(piv, ax) - mr;
+            int i0 = (int)(std::lower_bound(arr.begin(), arr.begin() + mid, lo, [&](int v, double c) { return X(v, ax) < c; }) -
+                           arr.begin());
+            for (int i = i0; i < mid && out.size() < limit; i++) {
                 int v = arr[i];
-                for (int p = gp[v]; p < gp[v + 1]; p++) {
-                    int w = gi[p];
-                    if (mark[w] == in_set && !less(w, piv, ax)) {
+                for (int p = gp[v]; p < gp[v + 1]; p++)
+                    if (mark[gi[p]] == in_set && !less(gi[p], piv, ax)) {
                         out.push_back(v);
                         break;
                     }
-                }
             }
         } else {
-            for (int i = mid; i < n && X(arr[i], ax) <= X(last, ax) + mr; i++) {
+            double hi = X(last, ax) + mr;
+            for (int i = mid; i < n && X(arr[i], ax) <= hi && out.size() < limit; i++) {
                 int v = arr[i];
-                for (int p = gp[v]; p < gp[v + 1]; p++) {
-                    int w = gi[p];
-                    if (mark[w] == in_set && less(w, piv, ax)) {
+                for (int p = gp[v]; p < gp[v + 1]; p++)
+                    if (mark[gi[p]] == in_set && less(gi[p], piv, ax)) {
                         out.push_back(v);
                         break;
                     }
-                }
             }
         }
     }
 
-    void split(std::vector<int> &set)  // set: ascending node ids
+    // Minimum vertex cover of the edges between side L and side R, with the separator S counted on side sside
+    // (0 left, 1 right): U = left nodes with a right neighbour, V = right nodes with a left neighbour; a maximum
+    // matching (greedy, then augmenting paths searched depth first, an explicit stack in place of recursion) and
+    // König's theorem give the cover (U minus Z) + (V in Z), Z the nodes reachable from unmatched U by
+    // alternating paths.
+    std::vector<int> cover(const std::vector<int> &L, const std::vector<int> &R, const std::vector<int> &S, int sL, int sR,
+                           int sside)
+    {
+        auto isL = [&](int v) { return mark[v] == sL || (mark[v] == -7 && sside == 0); };
+        auto isR = [&](int v) { return mark[v] == sR || (mark[v] == -7 && sside == 1); };
+        for (int v : S) mark[v] = -7;
+        std::vector<int> U, V;
+        auto classify = [&](const std::vector<int> &vs) {
+            for (int v : vs) {
+                bool l = isL(v);
+                for (int p = gp[v]; p < gp[v + 1]; p++) {
+                    int w = gi[p];
+                    if ((l && isR(w)) || (!l && isL(w))) {
+                        (l ? U : V).push_back(v);
+                        break;
+                    }
+                }
+            }
+        };
+        classify(L), classify(R), classify(S);
+        for (int i = 0; i < (int)V.size(); i++) loc[V[i]] = i;
+        std::vector<std::vector<int>> adj(U.size());
+        for (int i = 0; i < (int)U.size(); i++)
+            for (int p = gp[U[i]]; p < gp[U[i] + 1]; p++) {
+                int w = gi[p];
+                if (isR(w) && loc[w] >= 0) adj[i].push_back(loc[w]);
+            }
+        std::vector<int> mu(U.size(), -1), mv(V.size(), -1);
+        vis.assign(V.size(), -1);
+        for (int u = 0; u < (int)U.size(); u++)
+            for (int v : adj[u])
+                if (mv[v] < 0) {
+                    mu[u] = v, mv[v] = u;
+                    break;
+                }
+        std::vector<std::pair<int, int>> st;  // (u, next edge)
+        for (int u0 = 0; u0 < (int)U.size(); u0++) {
+            if (mu[u0] >= 0) continue;
+            st.assign(1, {u0, 0});
+            while (!st.empty()) {
+                auto &top = st.back();
+                int u = top.first;
+                if (top.second == (int)adj[u].size()) {
+                    st.pop_back();
+                    continue;
+                }
+                int v = adj[u][top.second++];
+                if (vis[v] == u0) continue;
+                vis[v] = u0;
+                if (mv[v] < 0) {  // augmenting path found: every frame takes the edge it last followed
+                    for (auto &f : st) {
+                        int vf = adj[f.first][f.second - 1];
+                        mu[f.first] = vf, mv[vf] = f.first;
+                    }
+                    break;
+                }
+                st.push_back({mv[v], 0});
+            }
+        }
+        std::vector<char> zu(U.size(), 0), zv(V.size(), 0);
+        std::vector<int> q;
+        for (int u = 0; u < (int)U.size(); u++)
+            if (mu[u] < 0) zu[u] = 1, q.push_back(u);
+        while (!q.empty()) {
+            int u = q.back();
+            q.pop_back();
+            for (int v : adj[u])
+                if (!zv[v]) {
+                    zv[v] = 1;
+                    int u2 = mv[v];
+                    if (u2 >= 0 && !zu[u2]) zu[u2] = 1, q.push_back(u2);
+                }
+        }
+        std::vector<int> C;
+        for (int u = 0; u < (int)U.size(); u++)
+            if (!zu[u]) C.push_back(U[u]);
+        for (int v = 0; v < (int)V.size(); v++)
+            if (zv[v]) C.push_back(V[v]);
+        for (int v : V) loc[v] = -1;
+        for (int v : S) mark[v] = sside == 0 ? sL : sR;
+        return C;
+    }
+
+    void split(std::vector<int> &set, int depth)
     {
         int n = (int)set.size();
         if (n <= kLeaf) {
@@ -90,8 +182,8 @@ struct CoordNd {
         for (int v : set) mark[v] = in_set;
         double best = 1e300;
         int best_ax = -1, best_mid = 0;
-        bool best_left = true;
-        std::vector<int> arr[3], bnd;
+        std::vector<int> arr[3], SL, SR, S;
+        bool s_left = true;
         for (int ax = 0; ax < 3; ax++) {
             arr[ax] = set;
             std::sort(arr[ax].begin(), arr[ax].end(), [&](int a, int b) { return less(a, b, ax); });
@@ -100,37 +192,49 @@ struct CoordNd {
             for (int f = 40; f <= 60; f += 5) {
                 int mid = (int)((int64_t)n * f / 100);
                 if (mid < 1 || mid >= n) continue;
-                for (int side = 0; side < 2; side++) {
-                    boundary(arr[ax], mid, ax, mr, side == 0, in_set, bnd);
-                    double s = (double)bnd.size();
-                    double big = side == 0 ? std::max(mid - s, (double)(n - mid)) : std::max((double)mid, n - mid - s);
-                    double cost = s * (1.0 + 2.0 * std::max(0.0, big / n - 0.5));
-                    if (cost < best) {
-                        best = cost, best_ax = ax, best_mid = mid, best_left = side == 0;
-                    }
-                }
+                // a boundary of `limit` nodes or more cannot beat the best cut so far (the penalty is >= 1)
+                size_t limit = best < 1e300 ? (size_t)best + 1 : SIZE_MAX;
+                boundary(arr[ax], mid, ax, mr, true, in_set, SL, limit);
+                boundary(arr[ax], mid, ax, mr, false, in_set, SR, limit);
+                bool useL = SL.size() <= SR.size();
+                const std::vector<int> &B = useL ? SL : SR;
+                double nl = mid - (useL ? (double)B.size() : 0), nr = (n - mid) - (useL ? 0 : (double)B.size());
+                double cost = B.size() * (1.0 + 2.0 * std::max(0.0, std::max(nl, nr) / n - 0.5));
+                if (cost < best) best = cost, best_ax = ax, best_mid = mid, s_left = useL, S = B;
             }
         }
-        boundary(arr[best_ax], best_mid, best_ax, [&] {
-            double mr = 0;
-            for (int v : set) mr = std::max(mr, reach[best_ax][v]);
-            return mr;
-        }(), best_left, in_set, bnd);
         int in_sep = ++stamp;
-        for (int v : bnd) mark[v] = in_sep;
+        for (int v : S) mark[v] = in_sep;
         std::vector<int> L, R;
         const std::vector<int> &a = arr[best_ax];
         for (int i = 0; i < n; i++)
             if (mark[a[i]] != in_sep) (i < best_mid ? L : R).push_back(a[i]);
-        std::sort(bnd.begin(), bnd.end());
-        std::sort(L.begin(), L.end());
-        std::sort(R.begin(), R.end());
-        for (int i = (int)bnd.size() - 1; i >= 0; i--) perm_rev.push_back(bnd[i]);
-        std::vector<int>().swap(arr[0]), std::vector<int>().swap(arr[1]), std::vector<int>().swap(arr[2]);
-        set.clear();
-        set.shrink_to_fit();
-        split(R);
-        split(L);
+        if (depth < kCoverDepth) {
+            int sL = ++stamp, sR = ++stamp;
+            for (int v : L) mark[v] = sL;
+            for (int v : R) mark[v] = sR;
+            std::vector<int> C0 = cover(L, R, S, sL, sR, 0), C1 = cover(L, R, S, sL, sR, 1);
+            int sside = C0.size() <= C1.size() ? 0 : 1;
+            std::vector<int> &C = sside == 0 ? C0 : C1;
+            if (C.size() < S.size()) {
+                int in_c = ++stamp;
+                for (int v : C) mark[v] = in_c;
+                std::vector<int> L2, R2;
+                for (int v : L)
+                    if (mark[v] != in_c) L2.push_back(v);
+                for (int v : R)
+                    if (mark[v] != in_c) R2.push_back(v);
+                for (int v : S)
+                    if (mark[v] != in_c) (sside == 0 ? L2 : R2).push_back(v);
+                S.swap(C), L.swap(L2), R.swap(R2);
+            }
+        }
+        (void)s_left;
+        for (int i = (int)S.size() - 1; i >= 0; i--) perm_rev.push_back(S[i]);
+        for (auto &v : arr) std::vector<int>().swap(v);
+        std::vector<int>().swap(set);
+        split(R, depth + 1);
+        split(L, depth + 1);
     }
 };
 }  // namespace

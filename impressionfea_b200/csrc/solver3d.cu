@@ -60,13 +60,14 @@ struct Forging3D {
     std::unique_ptr<LinearSolver> lin;
     // Symbolic analysis of the pattern, started on a host thread when the mesh is set and taken by the first
     // factorisation; the job reads only topo's pattern and node_xyz, which nothing writes meanwhile. Node order
-    // (`ordering`): 0 (default) METIS; 1 coordinate nested dissection (13 ms instead of 86 ms to compute on the
-    // 31.9k-tet case, about 7 % slower factorisations: a longer panel chain).
+    // (`ordering`): 1 (default) the library's coordinate nested dissection with minimum-vertex-cover separators
+    // at the top levels (21 ms instead of METIS's 86 ms on the 31.9k-tet case, and a shorter panel chain:
+    // 105 steps against 115); 0 METIS through cuSOLVER.
     std::thread sym_job;
     std::unique_ptr<MfSymbolic> sym_pre;
     std::string sym_err;
     double t_sym_wait = 0;
-    int ordering = 0;
+    int ordering = 1;
     std::vector<double> node_xyz;  // node coordinates when the mesh was set
     bool need_analyze = true, have_factor = false;
     // single-precision factor refined by FP64 PCG (off: the reference's FP64 direct solve after a factorisation)
