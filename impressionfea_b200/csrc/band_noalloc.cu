@@ -8,7 +8,6 @@
 // GPU that loads the library (kept until the process exits).
 #include <algorithm>
 #include <cstring>
-#include <mutex>
 
 #include "common.cuh"
 #include "runtime.cuh"
@@ -103,25 +102,15 @@ static __global__ void k_band_factor_solve_scratch(int n, int b, double *__restr
 }
 
 namespace {
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-double *g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of the scratch array for the current device, looked up once per device with it current.
+// Device address of the scratch array in the calling thread's current device context. Looked up on every call
+// (it allocates nothing and costs a driver query), so that a reset device or a new primary context never sees
+// an address from an earlier context.
 cudaError_t scratch_address(double **out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_band_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_band_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_ptr[dev] = (double *)p;
-    }
-    *out = g_scratch_ptr[dev];
+    *out = (double *)p;
     return cudaSuccess;
 }
 }  // namespace

@@ -2,9 +2,14 @@
 
 Callers whose device memory is owned by their own pooling allocator, or that run a solve inside a loop where
 cudaMalloc/cudaFree must not happen, hand in device buffers they already own; the entry point's only working
-memory is a fixed device array inside the library. This test calls it twice in a row through the C ABI (the
-array keeps the previous call's contents, so the second call checks nothing stale leaks in) and compares each
-result with ifea_band_factor_solve on the same system.
+memory is a fixed device array inside the library, shared by every call on a GPU and never cleared between them.
+These tests call it through the C ABI several times in a row and compare each result with ifea_band_factor_solve
+on the same system, bit for bit (both kernels subtract the products in the same order):
+
+- two successful calls in a row, the first with a half-bandwidth wide enough that only part of the band fits the
+  fixed array at once (the circular row window is reloaded as the factorisation walks down the band);
+- a call that fails on a non-positive pivot followed by a good call, so that the failed call's status words,
+  which stay in the array, must not leak into the next result.
 """
 import ctypes as C
 
@@ -16,7 +21,7 @@ from impressionfea_b200.forging2d import band_factor_solve
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 1e-12
+SCRATCH_DOUBLES = 262144 - 32  # row window capacity of the fixed array, in doubles
 
 
 def _spd_band(n, b, seed):
@@ -42,24 +47,35 @@ def _noalloc(a, rhs, b):
     row, piv = C.c_int32(7), C.c_double(7.0)
     stream = torch.cuda.current_stream().cuda_stream
     st = f(len(rhs), b, C.c_void_p(da.data_ptr()), C.c_void_p(dr.data_ptr()), C.byref(row), C.byref(piv), C.c_void_p(stream))
-    return st, row.value, da.cpu().numpy(), dr.cpu().numpy()
+    return st, row.value, piv.value, da.cpu().numpy(), dr.cpu().numpy()
+
+
+def _check_against_allocating_entry(n, b, seed, label):
+    a, rhs = _spd_band(n, b, seed)
+    L_ref, x_ref = band_factor_solve(a, b, rhs)
+    st, row, _, L_gpu, x_gpu = _noalloc(a, rhs, b)
+    assert st == 0 and row == -1, f"{label}: status {st}, row {row}"
+    np.testing.assert_array_equal(L_gpu, L_ref, err_msg=label)
+    np.testing.assert_array_equal(x_gpu, x_ref, err_msg=label)
 
 
 def test_noalloc_matches_allocating_entry_on_two_calls_in_a_row():
-    for call, (n, b, seed) in enumerate([(900, 85, 11), (400, 40, 12)]):
-        a, rhs = _spd_band(n, b, seed)
-        L_ref, x_ref = band_factor_solve(a, b, rhs)
-        st, row, L_gpu, x_gpu = _noalloc(a, rhs, b)
-        assert st == 0 and row == -1, f"call {call + 1}: status {st}, row {row}"
-        np.testing.assert_allclose(L_gpu, L_ref, rtol=RTOL, atol=0)
-        np.testing.assert_allclose(x_gpu, x_ref, rtol=RTOL, atol=1e-300)
+    # n = 3000, b = 160: the window holds 262112 // 161 = 1628 rows < n, so rows are reloaded into its slots
+    # (b = 160 also keeps the allocating entry point's shared-memory window, 161 rows of 161 doubles, in bounds).
+    assert SCRATCH_DOUBLES // 161 < 3000
+    _check_against_allocating_entry(3000, 160, 11, "call 1 (circular window)")
+    _check_against_allocating_entry(400, 40, 12, "call 2 (whole band in the window)")
 
 
-def test_noalloc_reports_non_positive_pivot_and_rejects_oversized_band():
+def test_noalloc_good_call_after_a_failed_one_reports_no_stale_status():
     a = np.zeros(3 * 2)
-    a[1], a[3], a[5] = 1.0, -1.0, 1.0
-    st, row, _, _ = _noalloc(a, np.ones(3), 1)
-    assert st == 4 and row == 1
+    a[1], a[3], a[5] = 1.0, -1.0, 1.0  # pivot of row 1 is -1 - 0 < 0
+    st, row, piv, _, _ = _noalloc(a, np.ones(3), 1)
+    assert st == 4 and row == 1 and piv == -1.0
+    _check_against_allocating_entry(900, 85, 13, "good call after a NOT_SPD call")
+
+
+def test_noalloc_rejects_a_band_wider_than_the_fixed_array():
     n, b = 600, 511  # (b + 1)^2 doubles exceed the fixed scratch array
-    st, _, _, _ = _noalloc(np.ones(n * (b + 1)), np.ones(n), b)
+    st, _, _, _, _ = _noalloc(np.ones(n * (b + 1)), np.ones(n), b)
     assert st == 1
