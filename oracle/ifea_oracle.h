@@ -76,11 +76,15 @@ int o3d_set_scalar(o3d *s, const char *name, double v);
 typedef struct ospd ospd;
 ospd *ospd_create(void);
 void ospd_destroy(ospd *f);
+/* optional: node coordinates (3 equations per node) for a coordinate nested-dissection order */
+void ospd_set_geometry(ospd *f, int nnodes, const double *xyz);
 int ospd_analyze(ospd *f, int n, const int32_t *col_ptr, const int32_t *row_idx);
 int ospd_factorize(ospd *f, const double *values);
 int ospd_solve(ospd *f, const double *b, double *x);
 int64_t ospd_factor_nonzeros(const ospd *f);
 int ospd_bad_pivot(const ospd *f);
+double ospd_factor_flops(const ospd *f);  /* multiply-adds of one factorisation */
+int ospd_supernodes(const ospd *f);
 
 /* ------------------------------------------------------------------ band Cholesky (SymmetricBandMatrix) */
 typedef struct oband oband;

@@ -833,13 +833,14 @@ static int solve_linear(o3d *s, const double *b, double *x)
         if (++s->pcg_failures >= 2) s->pcg_skip = imin(64, 1 << (s->pcg_failures - 1));
     }
     if (s->need_analyze) {
+        ospd_set_geometry(s->lin, s->nn, s->x);
         ospd_analyze(s->lin, s->ndof, s->col_ptr, s->row_idx);
         s->need_analyze = 0;
     }
     if (ospd_factorize(s->lin, s->val) != 0) {
         s->have_factor = 0;
         char msg[200];
-        snprintf(msg, sizeof msg, "Sparse factorisation failed at step %d (oracle up-looking Cholesky): not positive definite at equation %d.",
+        snprintf(msg, sizeof msg, "Sparse factorisation failed at step %d (oracle multifrontal Cholesky): not positive definite at equation %d.",
                  s->step_index, ospd_bad_pivot(s->lin));
         return -fail(s, E_DIVERGED, msg);
     }

@@ -48,23 +48,4 @@ double hf_height(const o_hfdie *d, double x, double y);
 double hf_clearance(const o_hfdie *d, v3 p, double offset);
 v3 hf_project(const o_hfdie *d, v3 p, double offset, v3 *normal);
 
-/* Sparse SPD factorisation used as the oracle's ISpdSolver backend. */
-struct ospd {
-    int n;
-    int nnz_full;
-    int32_t *ap, *ai;      /* full CSC pattern (copied) */
-    int *perm, *pinv;      /* fill-reducing order: new k = pinv[old] */
-    int32_t *cp, *ci;      /* upper triangle of the permuted matrix, CSC */
-    int *cmap;             /* cp/ci entry -> index into the full value array */
-    int *parent;           /* elimination tree */
-    int64_t *lp;           /* L column pointers */
-    int *li;
-    double *lx;
-    double *work;
-    int *stack, *mark;
-    int factored;
-    int bad_pivot;
-    int64_t lnz;
-};
-
 #endif

@@ -203,7 +203,7 @@ class Oracle3D:
 
 
 class OracleSpd:
-    """Oracle ISpdSolver backend: up-looking sparse Cholesky (stand-in for CSparse.NET)."""
+    """Oracle ISpdSolver backend: supernodal multifrontal Cholesky (stand-in for MKL PARDISO / CSparse.NET)."""
 
     def __init__(self):
         self.L = lib()
