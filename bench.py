@@ -38,15 +38,8 @@ TARGET_TETS = 30000
 
 
 def workload():
-    from impressionfea_b200.config import Forging3DConfig
-    from impressionfea_b200.meshes import h_for_tets, upset_case_3d
-
-    h = round(h_for_tets(R, H, TARGET_TETS), 3)
-    stroke = SHUT_RED * H
-    mesh, dies = upset_case_3d(R, H, h, shut=H - stroke, seed=2024)
-    cfg = Forging3DConfig(C=150, N=0.1, M=0.12, eps0=0.01, friction=0.4, ram=50.0, h=h, ds=stroke / STEPS_TOTAL,
-                          size=H, tol=1e-3)
-    return cfg, mesh, dies
+    from impressionfea_b200.workloads import upsetting_drop_in
+    return upsetting_drop_in()
 
 
 def config_dict(cfg, mesh, extra=None):
@@ -183,16 +176,8 @@ FAST_TOL = 2e-4  # Newton tolerance of the timed form: five times tighter than t
 
 
 def closed_die_workload():
-    """Closed-die gear blank (hub r15, web 6 mm, rim r45, flash gap 3 mm, land 3:1) as height
-    fields at dx = 0.5 mm, billet d40 x h50, ~205k tets, C=140, n=0.08, m=0.15, friction 0.3, 200 steps to closure."""
-    from impressionfea_b200.config import Forging3DConfig
-    from impressionfea_b200.meshes import gear_blank_case_3d, h_for_tets
-
-    h = round(h_for_tets(20.0, 50.0, 200000), 3)
-    mesh, dies = gear_blank_case_3d(h, seed=7, ramp=4.0)
-    cfg = Forging3DConfig(C=140, N=0.08, M=0.15, eps0=0.01, friction=0.3, ram=50.0, h=h, ds=mesh.gap0 / 200, size=50.0,
-                          tol=1e-3)
-    return cfg, mesh, dies
+    from impressionfea_b200.workloads import closed_die_gear_blank
+    return closed_die_gear_blank()
 
 
 def run_closed_die(stream, flush, warmup=2, steps=8):

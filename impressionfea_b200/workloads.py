@@ -1,0 +1,39 @@
+"""The forging cases the library is measured and checked on (synthetic inputs of the published configurations).
+
+- ``upsetting_drop_in()``: 3D upsetting, quarter model of a d30 x h45 billet, ~30k linear tets from a seeded
+  Delaunay fill (node jitter +-10 % of h), flat dies as two-triangle height fields, C = 150 MPa, eps0 = 0.01,
+  n = 0.1, m = 0.12, friction m_f = 0.4, 40 % reduction in 80 increments, ram 50 mm/s, tolerance 1e-3.
+- ``closed_die_gear_blank()``: closed-die forging of an axisymmetric gear blank (hub r15, web 6 mm, rim r45,
+  flash gap 3 mm, land 3:1) as two height fields at dx = 0.5 mm, billet d40 x h50, ~205k tets, C = 140 MPa,
+  n = 0.08, m = 0.15, friction 0.3, 200 increments to closure.
+- ``upsetting_2d()``: 2D axisymmetric upsetting, r10 x h30 billet, 20 x 60 quads, flat dies, C = 120 MPa,
+  eps0 = 0.01, n = 0.05, m = 0.15, friction 0.3, ram 10 mm/s, 50 % in 100 increments, tolerance 1e-6.
+
+The reference builds its 3D billets by isosurface stuffing (ThreeD/IsosurfaceStuffing.cs); here the same
+generated arrays feed the CUDA path and the oracle, which is all the per-iteration path consumes.
+"""
+from .config import Forging2DConfig, Forging3DConfig
+from .meshes import gear_blank_case_3d, h_for_tets, upset_case_3d
+
+UPSET_R, UPSET_H, UPSET_REDUCTION, UPSET_STEPS, UPSET_TETS = 15.0, 45.0, 0.40, 80, 30000
+
+
+def upsetting_drop_in(target_tets=UPSET_TETS, seed=2024):
+    h = round(h_for_tets(UPSET_R, UPSET_H, target_tets), 3)
+    stroke = UPSET_REDUCTION * UPSET_H
+    mesh, dies = upset_case_3d(UPSET_R, UPSET_H, h, shut=UPSET_H - stroke, seed=seed)
+    cfg = Forging3DConfig(C=150, N=0.1, M=0.12, eps0=0.01, friction=0.4, ram=50.0, h=h, ds=stroke / UPSET_STEPS,
+                          size=UPSET_H, tol=1e-3)
+    return cfg, mesh, dies
+
+
+def closed_die_gear_blank(target_tets=200000, seed=7):
+    h = round(h_for_tets(20.0, 50.0, target_tets), 3)
+    mesh, dies = gear_blank_case_3d(h, seed=seed, ramp=4.0)
+    cfg = Forging3DConfig(C=140, N=0.08, M=0.15, eps0=0.01, friction=0.3, ram=50.0, h=h, ds=mesh.gap0 / 200,
+                          size=50.0, tol=1e-3)
+    return cfg, mesh, dies
+
+
+def upsetting_2d():
+    return Forging2DConfig()

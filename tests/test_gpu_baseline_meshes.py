@@ -1,0 +1,224 @@
+"""Parity of the CUDA path with the oracle on the published workloads' own meshes, and on a sliver case.
+
+- 3D upsetting drop-in (31.9k tets): pattern, slot maps and contact flags bit-exact; one teacher-forced
+  PrepareStep bit-exact and one matrix assembly at 1e-12; then three increments with equal Newton iteration
+  counts, load / velocity / effective strain within 1e-6 relative and contact flags bit-exact.
+- Closed-die gear blank (205k tets, height-field dies with ramps): pattern and initial placement bit-exact;
+  PrepareStep bit-exact; one matrix assembly at 1e-12; one TryUpdate with the initial velocity field (die
+  clearance, projection and capture on the non-flat height fields: ThreeD/HeightFieldDie.cs:100-191,
+  ThreeD/Vec3.cs:34-56) with contact flags bit-exact; then the first increment (Newton iterations, load,
+  contact).
+- A small mesh with one planted sliver tet next to a contact node: TryUpdate runs ImprovePlacement and
+  SmoothInterior (Forging3DSolver.cs:1508-1510, :1625-1679, :1776-1838), and the RemeshTrigger's first-aid
+  smoothing (:1867-1883) runs at the start of the increment with the default remesh quality.
+- 2D axisymmetric upsetting (20 x 60 quads): 80 of its 100 increments, each with equal Newton iterations,
+  load within 1e-6, contact flags bit-exact; both paths then stop at the same increment with the same mesh
+  distortion (the reference remeshes there, which is outside this library).
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from impressionfea_b200 import _lib
+from impressionfea_b200.config import Forging3DConfig
+from impressionfea_b200.forging2d import ForgingSolver2D
+from impressionfea_b200.forging3d import Forging3DSolver
+from impressionfea_b200.meshes import upset_case_3d
+from impressionfea_b200.workloads import closed_die_gear_blank, upsetting_2d, upsetting_drop_in
+from oracle import Oracle2D, Oracle3D
+
+pytestmark = pytest.mark.gpu
+
+RTOL_ELEM = 1e-12
+RTOL_ENERGY = 1e-10
+RTOL_STATE = 1e-6
+
+
+def _close(a, b, rtol, what):
+    a = np.asarray(a, float)
+    b = np.asarray(b, float)
+    scale = max(np.abs(b).max(), 1e-300)
+    err = np.abs(a - b).max() / scale
+    assert err <= rtol, f"{what}: max abs diff / max |ref| = {err:.3e} > {rtol:.1e}"
+
+
+def _topology_bit_exact(gpu, ora):
+    cp, ri = gpu.pattern()
+    np.testing.assert_array_equal(cp, ora.array("col_ptr"))
+    np.testing.assert_array_equal(ri, ora.array("row_idx"))
+    for name in ("nbr_start", "nbr", "e_nbr", "bface", "is_surface", "contact"):
+        np.testing.assert_array_equal(gpu.array(name), ora.array(name), err_msg=name)
+    np.testing.assert_array_equal(gpu.array("x"), ora.array("x"), err_msg="initial placement")
+
+
+def _prepare_bit_exact(gpu, ora):
+    gpu.prepare_step()
+    ora.prepare_step()
+    for name in ("fixed", "n_fix", "die_axis", "ax", "grad", "vol", "v_node", "g_coef", "kvol"):
+        np.testing.assert_array_equal(gpu.array(name), ora.array(name), err_msg=name)
+    _close(gpu.array("a_fric"), ora.array("a_fric"), 0, "friction areas")
+    _close(gpu.array("v"), ora.array("v"), 0, "velocity guess")
+
+
+def _assembly_matches(gpu, ora):
+    v = ora.array("v") * (1 + 0.01 * np.sin(np.arange(len(ora.array("v")))))
+    eg, pg = gpu.assemble(1, 1, v)
+    eo, po = ora.assemble(1, 1, v)
+    assert abs(eg / eo - 1) < RTOL_ENERGY and abs(pg / po - 1) < RTOL_ENERGY
+    _close(gpu.array("val"), ora.array("val"), RTOL_ELEM, "assembled values")
+    _close(gpu.array("r"), ora.array("r"), 1e-11, "residual")
+    _close(gpu.array("el_sig"), ora.array("el_sig"), RTOL_ELEM, "element flow stress")
+
+
+def _increment_matches(gpu, ora, k):
+    info = gpu.step()
+    ora.step()
+    assert info["iterations"] == ora.scalar("iterations"), f"increment {k}: Newton iterations differ"
+    assert abs(info["load"] / ora.scalar("load") - 1) < RTOL_STATE, f"increment {k}: load"
+    np.testing.assert_array_equal(gpu.array("contact"), ora.array("contact"), err_msg=f"increment {k}: contact")
+    _close(gpu.array("vg"), ora.array("vg"), RTOL_STATE, f"increment {k}: velocity")
+    _close(gpu.array("eps"), ora.array("eps"), RTOL_STATE, f"increment {k}: effective strain")
+    _close(gpu.array("x"), ora.array("x"), 1e-9, f"increment {k}: coordinates")
+
+
+# ------------------------------------------------------------------ 3D upsetting drop-in (31.9k tets)
+
+def test_upsetting_drop_in_topology_prepare_and_assembly():
+    cfg, mesh, dies = upsetting_drop_in()
+    assert mesh.ne > 30000
+    gpu, ora = Forging3DSolver(cfg, mesh, dies), Oracle3D(cfg, mesh, dies)
+    _topology_bit_exact(gpu, ora)
+    _prepare_bit_exact(gpu, ora)
+    _assembly_matches(gpu, ora)
+    gpu.close()
+
+
+def test_upsetting_drop_in_increments_track_the_oracle():
+    cfg, mesh, dies = upsetting_drop_in()
+    gpu, ora = Forging3DSolver(cfg, mesh, dies), Oracle3D(cfg, mesh, dies)
+    for k in range(1, 4):
+        _increment_matches(gpu, ora, k)
+    gpu.close()
+
+
+# ------------------------------------------------------------------ closed-die gear blank (205k tets)
+
+@pytest.fixture(scope="module")
+def gear_blank():
+    return closed_die_gear_blank()
+
+
+def test_gear_blank_topology_prepare_assembly_and_update(gear_blank):
+    cfg, mesh, dies = gear_blank
+    assert mesh.ne > 200000 and dies[0].nx > 100
+    gpu, ora = Forging3DSolver(cfg, mesh, dies), Oracle3D(cfg, mesh, dies)
+    _topology_bit_exact(gpu, ora)
+    _prepare_bit_exact(gpu, ora)
+    _assembly_matches(gpu, ora)
+    dt = cfg.ds / cfg.ram
+    assert gpu.try_update(dt) == ora.try_update(dt)
+    np.testing.assert_array_equal(gpu.array("contact"), ora.array("contact"), err_msg="contact after TryUpdate")
+    _close(gpu.array("x"), ora.array("x"), 1e-12, "coordinates after TryUpdate")
+    assert gpu.scalar("projection_reverts") == ora.scalar("projection_reverts")
+    gpu.close()
+
+
+def test_gear_blank_first_increment_tracks_the_oracle(gear_blank):
+    cfg, mesh, dies = gear_blank
+    gpu, ora = Forging3DSolver(cfg, mesh, dies), Oracle3D(cfg, mesh, dies)
+    _increment_matches(gpu, ora, 1)
+    gpu.close()
+
+
+# ------------------------------------------------------------------ sliver next to a contact node
+
+def _quality(x, t):
+    a, b, c, d = (x[t[:, i]] for i in range(4))
+    vol = np.einsum("ij,ij->i", b - a, np.cross(c - a, d - a)) / 6
+    l2 = (((b - a) ** 2).sum(1) + ((c - a) ** 2).sum(1) + ((d - a) ** 2).sum(1) + ((c - b) ** 2).sum(1)
+          + ((d - b) ** 2).sum(1) + ((d - c) ** 2).sum(1)) / 6
+    return 6 * np.sqrt(2) * vol / l2 ** 1.5
+
+
+def _sliver_case():
+    """Quarter cylinder r10 x h20 with one interior node moved 97 % of the way to the opposite face of a tet that
+    touches a top-die contact node (quality 0.029; every other tet of that node stays above 0.3)."""
+    mesh, dies = upset_case_3d(10.0, 20.0, 2.0, 12.0, seed=1)
+    cfg = Forging3DConfig(C=150, N=0.1, M=0.12, eps0=0.01, friction=0.3, ram=10, h=2.0, ds=0.2, size=20.0, tol=1e-6)
+    probe = Oracle3D(cfg, mesh, dies)
+    contact, surf = probe.array("contact"), probe.array("is_surface")
+    probe.close()
+    x, t = mesh.x.copy(), mesh.tets
+    tets_of = [[] for _ in range(len(x))]
+    for e, tt in enumerate(t):
+        for n in tt:
+            tets_of[n].append(e)
+    for e in range(len(t)):
+        if not any(contact[n] > 0 for n in t[e]):
+            continue
+        for a in range(4):
+            n = t[e][a]
+            if surf[n]:
+                continue
+            p0, p1, p2 = x[[t[e][b] for b in range(4) if b != a]]
+            nrm = np.cross(p1 - p0, p2 - p0)
+            nrm /= np.linalg.norm(nrm)
+            dist = np.dot(x[n] - p0, nrm)
+            xx = x.copy()
+            xx[n] = x[n] - 0.97 * dist * nrm
+            q = _quality(xx, t[tets_of[n]])
+            qe = _quality(xx, t[[e]])[0]
+            others = [qq for ee, qq in zip(tets_of[n], q) if ee != e]
+            if 0.015 < qe < 0.04 and min(others) > 0.1:
+                mesh.x = xx
+                return cfg, mesh, dies, e
+    raise AssertionError("no sliver placement found")
+
+
+@pytest.mark.parametrize("remesh_quality", [0.01, 0.12])
+def test_sliver_drives_improve_placement_and_smooth_interior(remesh_quality):
+    # remesh_quality 0.01: the sliver survives the RemeshTrigger, so TryUpdate meets a predicted tet below 0.05
+    # and runs ImprovePlacement over its contact nodes, then SmoothInterior over its interior node;
+    # 0.12 (the reference default): the RemeshTrigger's SmoothInterior repairs it before the Newton iteration.
+    cfg, mesh, dies, e = _sliver_case()
+    cfg = dataclasses.replace(cfg, remesh_quality=remesh_quality)
+    q0 = _quality(mesh.x, mesh.tets[[e]])[0]
+    gpu, ora = Forging3DSolver(cfg, mesh, dies), Oracle3D(cfg, mesh, dies)
+    for k in range(1, 3):
+        _increment_matches(gpu, ora, k)
+        for name in ("projection_reverts", "corner_penetrations", "remesh_requests"):
+            assert gpu.scalar(name) == ora.scalar(name), f"increment {k}: {name}"
+    q1 = _quality(gpu.array("x").reshape(-1, 3), mesh.tets[[e]])[0]
+    assert q1 > 0.05 > q0, f"the sliver was not repaired: {q0:.3f} -> {q1:.3f}"
+    gpu.close()
+
+
+# ------------------------------------------------------------------ 2D axisymmetric upsetting (20 x 60 quads)
+
+def test_2d_upsetting_80_increments_track_the_oracle():
+    cfg = upsetting_2d()
+    g, o = ForgingSolver2D(cfg), Oracle2D(cfg)
+    for k in range(1, 81):
+        info = g.step()
+        o.step()
+        assert info["iterations"] == o.scalar("iterations"), f"increment {k}"
+        assert abs(info["load"] / o.scalar("load") - 1) < RTOL_STATE, f"increment {k}: load"
+        np.testing.assert_array_equal(g.array("contact"), o.array("contact"), err_msg=f"increment {k}")
+        _close(g.array("x"), o.array("x"), 1e-9, f"increment {k}: coordinates")
+        _close(g.array("eps"), o.array("eps"), RTOL_STATE, f"increment {k}: strain")
+    # both stop at the same later increment on the same mesh distortion
+    stop_gpu = stop_ora = None
+    for k in range(81, 101):
+        if stop_gpu is None:
+            try:
+                g.step()
+            except _lib.MeshDistortionError:
+                stop_gpu = k
+        if stop_ora is None:
+            try:
+                o.step()
+            except RuntimeError as err:
+                assert "distortion" in str(err).lower()
+                stop_ora = k
+    assert stop_gpu == stop_ora
