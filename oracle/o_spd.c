@@ -159,8 +159,9 @@ static void nd_order(const o_graph *g, int *part, int *level, int *order, int *p
  * When the caller gives node coordinates (3 equations per node, DOF = 3 node + c), the order is a recursive
  * coordinate bisection of the node graph (George 1973, nested dissection of grids; its geometric form as in
  * Miller, Teng, Thurston and Vavasis 1998): the nodes are split at the median along the longest extent of their
- * bounding box, the smaller of the two one-sided boundary sets becomes the separator, numbered after both
- * halves; a node's three equations stay consecutive. */
+ * bounding box; the separator, numbered after both halves, is a minimum vertex cover of the edges between the
+ * halves (for more than 256 nodes) or the smaller of the two one-sided boundary sets; a node's three equations
+ * stay consecutive. */
 
 typedef struct {
     const double *xyz;
@@ -177,8 +178,83 @@ static int cmp_axis(const void *a, const void *b)
     return (u > v) - (u < v);
 }
 
-static void coord_nd(const int *np, const int *nj, const double *xyz, int *side, int *nodes, int cnt, int *out,
-                     int *nout)
+/* Minimum vertex cover of the bipartite cut graph between the boundary sets of two halves (König's theorem
+ * on a maximum matching from Hopcroft and Karp 1973). ua[] / ub[] are the boundary nodes of either half;
+ * adjacency from ua to ub in (ap, aj) over local indices. On return in_cover_a[i] / in_cover_b[j] mark the cover. */
+static void min_vertex_cover(int na, int nb, const int *ap, const int *aj, char *in_cover_a, char *in_cover_b)
+{
+    int *mate_a = (int *)malloc(sizeof(int) * (na > 0 ? na : 1)), *mate_b = (int *)malloc(sizeof(int) * (nb > 0 ? nb : 1));
+    int *dist = (int *)malloc(sizeof(int) * (na > 0 ? na : 1)), *queue = (int *)malloc(sizeof(int) * (na > 0 ? na : 1));
+    int *stk = (int *)malloc(sizeof(int) * (na > 0 ? na : 1)), *it = (int *)malloc(sizeof(int) * (na > 0 ? na : 1));
+    for (int i = 0; i < na; i++) mate_a[i] = -1;
+    for (int j = 0; j < nb; j++) mate_b[j] = -1;
+    for (;;) {
+        /* BFS layers from the free vertices of side a */
+        int head = 0, tail = 0, found = 0;
+        for (int i = 0; i < na; i++) {
+            if (mate_a[i] < 0) { dist[i] = 0; queue[tail++] = i; }
+            else dist[i] = -1;
+        }
+        while (head < tail) {
+            int i = queue[head++];
+            for (int p = ap[i]; p < ap[i + 1]; p++) {
+                int j = aj[p], i2 = mate_b[j];
+                if (i2 < 0) found = 1;
+                else if (dist[i2] < 0) { dist[i2] = dist[i] + 1; queue[tail++] = i2; }
+            }
+        }
+        if (!found) break;
+        /* DFS along the layers (iterative), one augmenting path per free vertex */
+        int augmented = 0;
+        for (int r = 0; r < na; r++) {
+            if (mate_a[r] >= 0 || dist[r] != 0) continue;
+            int top = 0;
+            stk[top++] = r;
+            it[r] = ap[r];
+            int end_j = -1;
+            while (top > 0 && end_j < 0) {
+                int i = stk[top - 1];
+                if (it[i] >= ap[i + 1]) { dist[i] = -1; top--; continue; }
+                int j = aj[it[i]++], i2 = mate_b[j];
+                if (i2 < 0) { end_j = j; break; }
+                if (dist[i2] == dist[i] + 1) { it[i2] = ap[i2]; stk[top++] = i2; }
+            }
+            if (end_j < 0) continue;
+            /* flip the path: stk[0..top-1] are side-a vertices, each matched to the b vertex it stepped through */
+            int j = end_j;
+            for (int q = top - 1; q >= 0; q--) {
+                int i = stk[q];
+                int prev = mate_a[i];
+                mate_a[i] = j;
+                mate_b[j] = i;
+                j = prev;
+            }
+            augmented++;
+        }
+        if (!augmented) break;
+    }
+    /* König: Z = vertices reachable from free side-a vertices by alternating paths */
+    char *za = (char *)calloc((size_t)(na > 0 ? na : 1), 1), *zb = (char *)calloc((size_t)(nb > 0 ? nb : 1), 1);
+    int head = 0, tail = 0;
+    for (int i = 0; i < na; i++)
+        if (mate_a[i] < 0) { za[i] = 1; queue[tail++] = i; }
+    while (head < tail) {
+        int i = queue[head++];
+        for (int p = ap[i]; p < ap[i + 1]; p++) {
+            int j = aj[p];
+            if (zb[j]) continue;
+            zb[j] = 1;
+            int i2 = mate_b[j];
+            if (i2 >= 0 && !za[i2]) { za[i2] = 1; queue[tail++] = i2; }
+        }
+    }
+    for (int i = 0; i < na; i++) in_cover_a[i] = !za[i];
+    for (int j = 0; j < nb; j++) in_cover_b[j] = zb[j];
+    free(za); free(zb); free(mate_a); free(mate_b); free(dist); free(queue); free(stk); free(it);
+}
+
+static void coord_nd(const int *np, const int *nj, const double *xyz, int *side, int *loc, int *nodes, int cnt,
+                     int *out, int *nout)
 {
     if (cnt <= 64) {
         for (int k = 0; k < cnt; k++) out[(*nout)++] = nodes[k];
@@ -212,23 +288,62 @@ static void coord_nd(const int *np, const int *nj, const double *xyz, int *side,
             else nb_b++;
         }
     }
-    int sep_side = na_b <= nb_b ? 1 : 2;
     int *a = (int *)malloc(sizeof(int) * cnt), *b = (int *)malloc(sizeof(int) * cnt), *s = (int *)malloc(sizeof(int) * cnt);
     int na = 0, nb = 0, ns = 0;
-    for (int k = 0; k < cnt; k++) {
-        int u = nodes[k], su = side[u], touch = 0;
-        if (su == sep_side)
+    if (cnt > 256) {
+        /* separator = a minimum vertex cover of the cut edges */
+        int *ua = (int *)malloc(sizeof(int) * (na_b > 0 ? na_b : 1)), *ub = (int *)malloc(sizeof(int) * (nb_b > 0 ? nb_b : 1));
+        int ka = 0, kb = 0;
+        for (int k = 0; k < cnt; k++) {
+            int u = nodes[k], su = side[u], touch = 0;
             for (int p = np[u]; p < np[u + 1] && !touch; p++) {
                 int w = nj[p];
                 if (side[w] != 0 && side[w] != su) touch = 1;
             }
-        if (touch) s[ns++] = u;
-        else if (su == 1) a[na++] = u;
-        else b[nb++] = u;
+            if (!touch) continue;
+            if (su == 1) { loc[u] = ka; ua[ka++] = u; }
+            else { loc[u] = kb; ub[kb++] = u; }
+        }
+        int *ap = (int *)malloc(sizeof(int) * (ka + 1));
+        ap[0] = 0;
+        for (int i = 0; i < ka; i++) {
+            int c = 0;
+            for (int p = np[ua[i]]; p < np[ua[i] + 1]; p++) c += side[nj[p]] == 2;
+            ap[i + 1] = ap[i] + c;
+        }
+        int *aj = (int *)malloc(sizeof(int) * (ap[ka] > 0 ? ap[ka] : 1));
+        for (int i = 0, q = 0; i < ka; i++)
+            for (int p = np[ua[i]]; p < np[ua[i] + 1]; p++)
+                if (side[nj[p]] == 2) aj[q++] = loc[nj[p]];
+        char *ca = (char *)malloc((size_t)(ka > 0 ? ka : 1)), *cb = (char *)malloc((size_t)(kb > 0 ? kb : 1));
+        min_vertex_cover(ka, kb, ap, aj, ca, cb);
+        for (int i = 0; i < ka; i++) if (ca[i]) side[ua[i]] = 3;
+        for (int j = 0; j < kb; j++) if (cb[j]) side[ub[j]] = 3;
+        free(ua); free(ub); free(ap); free(aj); free(ca); free(cb);
+        for (int k = 0; k < cnt; k++) {
+            int u = nodes[k];
+            if (side[u] == 3) s[ns++] = u;
+            else if (side[u] == 1) a[na++] = u;
+            else b[nb++] = u;
+        }
+    } else {
+        /* separator = the smaller one-sided boundary */
+        int sep_side = na_b <= nb_b ? 1 : 2;
+        for (int k = 0; k < cnt; k++) {
+            int u = nodes[k], su = side[u], touch = 0;
+            if (su == sep_side)
+                for (int p = np[u]; p < np[u + 1] && !touch; p++) {
+                    int w = nj[p];
+                    if (side[w] != 0 && side[w] != su) touch = 1;
+                }
+            if (touch) s[ns++] = u;
+            else if (su == 1) a[na++] = u;
+            else b[nb++] = u;
+        }
     }
     for (int k = 0; k < cnt; k++) side[nodes[k]] = 0;
-    coord_nd(np, nj, xyz, side, a, na, out, nout);
-    coord_nd(np, nj, xyz, side, b, nb, out, nout);
+    coord_nd(np, nj, xyz, side, loc, a, na, out, nout);
+    coord_nd(np, nj, xyz, side, loc, b, nb, out, nout);
     for (int k = 0; k < ns; k++) out[(*nout)++] = s[k];
     free(a);
     free(b);
@@ -255,10 +370,11 @@ static int coord_order(int n, const int32_t *col_ptr, const int32_t *row_idx, in
             if (row_idx[p] % 3 == 0 && row_idx[p] / 3 != u) nj[q++] = row_idx[p] / 3;
     }
     int *side = (int *)calloc((size_t)nnodes, sizeof(int)), *nodes = (int *)malloc(sizeof(int) * nnodes);
-    int *out = (int *)malloc(sizeof(int) * nnodes);
+    int *out = (int *)malloc(sizeof(int) * nnodes), *loc = (int *)malloc(sizeof(int) * nnodes);
     for (int u = 0; u < nnodes; u++) nodes[u] = u;
     int nout = 0;
-    coord_nd(np, nj, xyz, side, nodes, nnodes, out, &nout);
+    coord_nd(np, nj, xyz, side, loc, nodes, nnodes, out, &nout);
+    free(loc);
     for (int k = 0; k < nnodes; k++)
         for (int c = 0; c < 3; c++) perm[3 * k + c] = 3 * out[k] + c;
     free(np); free(nj); free(side); free(nodes); free(out);
