@@ -63,6 +63,7 @@ class StepInfo(C.Structure):
 
 _vp, _dp, _i32p, _u8p, _i64p = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_uint8), C.POINTER(C.c_int64)
 _st = C.c_int
+_fp = C.POINTER(C.c_float)
 
 SIGNATURES = {
     "ifea3d_create": (_st, [C.POINTER(Params3D), C.POINTER(_vp)]),
@@ -108,6 +109,22 @@ SIGNATURES = {
     "ifea_band_factor_solve": (_st, [C.c_int32, C.c_int32, _dp, _dp, _i32p, _dp]),
     "ifea_band_factor_solve_noalloc": (_st, [C.c_int32, C.c_int32, _vp, _vp, _i32p, _dp, _vp]),
     "ifea_version": (C.c_char_p, []),
+    "ifea_mlp_create": (_st, [C.c_uint64, C.POINTER(_vp)]),
+    "ifea_mlp_destroy": (None, [_vp]),
+    "ifea_mlp_last_error": (C.c_char_p, [_vp]),
+    "ifea_mlp_param_count": (C.c_int64, []),
+    "ifea_mlp_get_params": (_st, [_vp, _fp, C.c_int64]),
+    "ifea_mlp_set_params": (_st, [_vp, _fp, C.c_int64]),
+    "ifea_mlp_get_normalisation": (_st, [_vp, _fp]),
+    "ifea_mlp_set_normalisation": (_st, [_vp, _fp]),
+    "ifea_mlp_add_samples": (_st, [_vp, _fp, _fp, C.c_int64]),
+    "ifea_mlp_samples": (C.c_int64, [_vp]),
+    "ifea_mlp_clear_samples": (_st, [_vp]),
+    "ifea_mlp_fit_normalisation": (_st, [_vp]),
+    "ifea_mlp_forward": (_st, [_vp, _fp, C.c_int64, _fp]),
+    "ifea_mlp_gradients": (_st, [_vp, _fp, _fp, C.c_int64, _fp, _fp]),
+    "ifea_mlp_train": (_st, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _fp, _dp]),
+    "ifea3d_set_warm_start": (_st, [_vp, _vp, C.c_int32]),
 }
 
 _LIB = None

@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libifea_gpu.so")
-SOURCES = ["solver3d.cu", "solver2d.cu", "spd_capi.cu", "mesh3d.cpp", "mesh2d.cpp", "multifrontal.cpp", "band_noalloc.cu"]
+SOURCES = ["solver3d.cu", "solver2d.cu", "spd_capi.cu", "mesh3d.cpp", "mesh2d.cpp", "multifrontal.cpp", "band_noalloc.cu", "mlp.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -27,9 +27,9 @@ def _deps():
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(d) for d in _deps()):
         return LIB
-    objs = []
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
+    jobs = []
     for s in SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(objdir, s + ".o")
@@ -37,8 +37,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
                                "-Xcompiler", "-Wall", "-Xcompiler", "-Wno-deprecated-declarations", "-diag-suppress", "128", "-c", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        subprocess.check_call(cmd)
-        objs.append(obj)
+        jobs.append((cmd, obj))
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as pool:
+        for f in [pool.submit(subprocess.check_call, c) for c, _ in jobs]:
+            f.result()
+    objs = [o for _, o in jobs]
     cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcusolver", "-lcusparse", "-lcublas"]
     subprocess.check_call(cmd)
     return LIB

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "warmstart.h"
 #include "kernels3d.cuh"
 #include "mesh3d.h"
 #include "runtime.cuh"
@@ -34,6 +35,76 @@ static std::string fmt(const char *f, ...)
 
 // Adds the wall time of a scope to an accumulator (the phases end in a stream synchronisation, so host time
 // is the phase's time); the split mirrors Forging3DSolver.TimingSummary (:1924-1943).
+// ------------------------------------------------------------------ learned warm start (inputs, targets, guess)
+// The network replaces LoadVelocityGuess (Forging3DSolver.cs:854-869): from each node's state at the start of
+// an increment it predicts the change of the node's global velocity over the increment. Its 16 inputs per node
+// (FP32): the previous converged velocity and its change over the increment before (both / ram); the node's
+// mean effective strain and mean strain rate (/ the reference rate) over its tets; the contact state as one-hot
+// (free, bottom die, top die); the clearances to both dies (/ h, clamped to [-1, 4]); the stroke increment (/ h);
+// the radial and axial position (/ the billet size). v0 keeps the velocity the prediction is added to.
+__global__ void k_ws_features(View3 V, float *__restrict__ F, double *__restrict__ v0, double rate_ref, double h,
+                              double ds, double size, int have_prev)
+{
+    GRID_STRIDE(n, V.nn)
+    {
+        d3 g = ld3(V.vg, n), gp = have_prev ? ld3(V.vg_prev, n) : g;
+        st3(v0, n, g);
+        double e = 0, r = 0;
+        int cnt = V.nts[n + 1] - V.nts[n];
+        for (int32_t q = V.nts[n]; q < V.nts[n + 1]; q++) {
+            int t = V.ntl[q];
+            e += V.eps[t];
+            r += V.el_rate[t];
+        }
+        if (cnt) {
+            e /= cnt;
+            r /= cnt;
+        }
+        d3 p = ld3(V.x, n);
+        double cb = hf_clearance(V.die[0], p, 0), ct = hf_clearance(V.die[1], p, V.gap);
+        int c = V.contact[n];
+        float *f = F + 16 * (int64_t)n;
+        f[0] = (float)(g.x / V.ram); f[1] = (float)(g.y / V.ram); f[2] = (float)(g.z / V.ram);
+        f[3] = (float)((g.x - gp.x) / V.ram); f[4] = (float)((g.y - gp.y) / V.ram); f[5] = (float)((g.z - gp.z) / V.ram);
+        f[6] = (float)e;
+        f[7] = (float)(r / rate_ref);
+        f[8] = c == IFEA_FREE; f[9] = c == IFEA_BOTTOM_DIE; f[10] = c == IFEA_TOP_DIE;
+        f[11] = (float)rclamp(cb / h, -1.0, 4.0);
+        f[12] = (float)rclamp(ct / h, -1.0, 4.0);
+        f[13] = (float)(ds / h);
+        f[14] = (float)(sqrt(p.x * p.x + p.y * p.y) / size);
+        f[15] = (float)(p.z / size);
+    }
+}
+
+// training target of an accepted increment: the change of the global velocity over it, / ram
+__global__ void k_ws_targets(View3 V, const double *__restrict__ v0, float *__restrict__ T)
+{
+    GRID_STRIDE(n, V.nn)
+    {
+        d3 g = ld3(V.vg, n), a = ld3(v0, n);
+        T[3 * (int64_t)n] = (float)((g.x - a.x) / V.ram);
+        T[3 * (int64_t)n + 1] = (float)((g.y - a.y) / V.ram);
+        T[3 * (int64_t)n + 2] = (float)((g.z - a.z) / V.ram);
+    }
+}
+
+// the predicted start: v0 + ram * prediction, in the nodal frames, fixed DOFs overwritten (as k_guess)
+__global__ void k_ws_guess(View3 V, const double *__restrict__ v0, const float *__restrict__ Y, double *__restrict__ out)
+{
+    GRID_STRIDE(n, V.nn)
+    {
+        d3 a = ld3(v0, n);
+        d3 g = mk3(a.x + V.ram * (double)Y[3 * (int64_t)n], a.y + V.ram * (double)Y[3 * (int64_t)n + 1],
+                   a.z + V.ram * (double)Y[3 * (int64_t)n + 2]);
+        d3 l = to_local(V, n, g);
+        for (int c = 0; c < 3; c++) {
+            int d = 3 * n + c;
+            out[d] = V.fixed[d] ? V.fixed_val[d] : get3(l, c);
+        }
+    }
+}
+
 struct PhaseTimer {
     double &acc;
     std::chrono::steady_clock::time_point t0;
@@ -79,6 +150,13 @@ struct Forging3D {
     bool pcg_early_abort = false;
     int factor_step = -1, stale_failures = 0;  // increment of the cached factor; failed tries of a stale one
     int wide_rows = mf::kWideM;  // fronts at least this tall use the multi-CTA solve path
+    // learned warm start: mode bit 1 records (inputs, target) of every accepted increment into the network's
+    // training set, bit 2 starts each increment from the network's prediction when its energy is lower than
+    // the reference start's (else the reference start is kept)
+    WarmStartNet *ws_net = nullptr;
+    int ws_mode = 0, ws_used = 0, ws_fallbacks = 0;
+    DBuf<float> d_wsf, d_wst, d_wsy;
+    DBuf<double> d_wsv0;
     int pcg_failures = 0, pcg_skip = 0, pcg_failures_total = 0;
     // mesh
     TetTopology topo;
@@ -403,6 +481,38 @@ struct Forging3D {
         int trend = P.extrapolate_start && warm && have_vg_prev;
         k_guess<<<grid(topo.nn), 256, 0, st>>>(V, trend);
         cuda_check(cudaGetLastError(), "prepare_step launch");
+        if (ws_net && ws_mode) warm_start_guess();
+    }
+
+    void warm_start_guess()
+    {
+        int nn = topo.nn;
+        d_wsf.resize((size_t)16 * nn);
+        d_wsv0.resize((size_t)3 * nn);
+        View3 V = view();
+        k_ws_features<<<grid(nn), 256, 0, st>>>(V, d_wsf, d_wsv0, rate_ref, h, P.ds, P.size, have_vg_prev ? 1 : 0);
+        if (!(ws_mode & 2) || !warm || !have_vg_prev) return;
+        d_wsy.resize((size_t)3 * nn);
+        ws_net->infer_device(d_wsf, nn, d_wsy, st);
+        // keep whichever start has the lower value of the functional (the Newton iteration minimises it)
+        double e_ref = assemble(ASM_ENERGY, 0, d_vbuf[vcur], false, nullptr);
+        k_ws_guess<<<grid(nn), 256, 0, st>>>(V, d_wsv0, d_wsy, d_vbuf[1 - vcur]);
+        double e_net = assemble(ASM_ENERGY, 0, d_vbuf[1 - vcur], false, nullptr);
+        if (e_net < e_ref) {
+            vcur = 1 - vcur;
+            ws_used++;
+        } else {
+            ws_fallbacks++;
+        }
+    }
+
+    void warm_start_record()
+    {
+        if (!ws_net || !(ws_mode & 1) || d_wsv0.n != (size_t)3 * topo.nn) return;
+        d_wst.resize((size_t)3 * topo.nn);
+        View3 V = view();
+        k_ws_targets<<<grid(topo.nn), 256, 0, st>>>(V, d_wsv0, d_wst);
+        ws_net->add_samples_device(d_wsf, d_wst, topo.nn, st);
     }
 
     // ---------------------------------------------------------------- Assemble (:1115-1217)
@@ -769,6 +879,7 @@ struct Forging3D {
             double used = P.ram * dt;
             ds_cur = used_cutback > 0 ? rmax(used, step_cap / (1 << P.max_cutbacks)) : rmin(step_cap, 1.5 * ds_cur);
         }
+        warm_start_record();
         View3 V = view();
         k_strain_damage<<<grid(topo.ne), 256, 0, st>>>(V, dt);
         warm = 1;
@@ -841,6 +952,7 @@ struct Forging3D {
         S("t_graph_solve", lin->setup_s(3)) S("factor_gpu_ms", lin->factor_ms()) S("solve_gpu_ms", lin->solve_ms()) S("solves", lin->solves())
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
         S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows) S("tc_updates", lin->tc_launches())
+        S("ws_used", ws_used) S("ws_fallbacks", ws_fallbacks) S("ws_mode", ws_mode)
 #undef S
         if (nm == "volume") return volume();
         if (nm == "min_quality") return min_quality(d_x);
@@ -1032,6 +1144,15 @@ ifea_status ifea3d_try_update(ifea3d *ctx, double dt, int32_t *ok)
 ifea_status ifea3d_set_stream(ifea3d *ctx, void *cuda_stream)
 {
     return guarded(ctx, [&](Forging3D &s) { s.set_stream((cudaStream_t)cuda_stream); });
+}
+
+ifea_status ifea3d_set_warm_start(ifea3d *ctx, ifea_mlp *mlp, int32_t mode)
+{
+    if (mode < 0 || mode > 3 || (mode && (!mlp || !mlp->net))) return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) {
+        s.ws_net = mode ? mlp->net : nullptr;
+        s.ws_mode = mode;
+    });
 }
 
 ifea_status ifea3d_set_warm(ifea3d *ctx, int32_t warm)

@@ -151,6 +151,45 @@ ifea_status ifea_spd_solve(ifea_spd *s, const double *b, double *x);
 int64_t ifea_spd_factor_nonzeros(const ifea_spd *s);
 const char *ifea_spd_name(const ifea_spd *s);
 
+/* ------------------------------------------------------------------ learned warm start (3D)
+ *
+ * Replaces the initial velocity guess of each increment, LoadVelocityGuess (ThreeD/Forging3DSolver.cs:854-869:
+ * the previous increment's velocity in the nodal frames; ExtrapolateStart, :43-44 and :861-866, adds its trend).
+ * A per-node MLP, 16 inputs -> 3 hidden layers of 128 (GELU) -> 3 outputs, predicts the change of each node's
+ * global velocity over the coming increment from the node's state (previous velocity and its trend, mean
+ * effective strain and strain rate, contact state, die clearances, stroke increment, position). BF16 weights and
+ * activations, FP32 accumulation on the tensor cores; FP32 master weights trained by Adam on samples the solver
+ * records from its own converged increments. The reference has no counterpart beyond the guess it replaces. */
+typedef struct ifea_mlp ifea_mlp;
+ifea_status ifea_mlp_create(uint64_t seed, ifea_mlp **out);   /* seeded He-uniform weights, zero biases */
+void ifea_mlp_destroy(ifea_mlp *m);
+const char *ifea_mlp_last_error(const ifea_mlp *m);
+int64_t ifea_mlp_param_count(void);                              /* FP32 parameters: W1 b1 W2 b2 W3 b3 W4 b4 */
+ifea_status ifea_mlp_get_params(ifea_mlp *m, float *params, int64_t count);
+ifea_status ifea_mlp_set_params(ifea_mlp *m, const float *params, int64_t count);   /* resets Adam's moments */
+/* input mean[16], input std[16], output mean[3], output std[3] */
+ifea_status ifea_mlp_get_normalisation(ifea_mlp *m, float *norm38);
+ifea_status ifea_mlp_set_normalisation(ifea_mlp *m, const float *norm38);
+/* training set: raw inputs [n][16] and raw targets [n][3] (host arrays) */
+ifea_status ifea_mlp_add_samples(ifea_mlp *m, const float *inputs, const float *targets, int64_t n);
+int64_t ifea_mlp_samples(const ifea_mlp *m);
+ifea_status ifea_mlp_clear_samples(ifea_mlp *m);
+ifea_status ifea_mlp_fit_normalisation(ifea_mlp *m);             /* mean / std of the training set */
+/* raw outputs [n][3] for raw inputs [n][16] (host arrays) */
+ifea_status ifea_mlp_forward(ifea_mlp *m, const float *inputs, int64_t n, float *outputs);
+/* gradient of the mean squared error over the normalised targets at the current parameters, n rows (a multiple
+ * of 128, at most 8192); grad gets ifea_mlp_param_count() values */
+ifea_status ifea_mlp_gradients(ifea_mlp *m, const float *inputs, const float *targets, int64_t n, float *grad,
+                               float *loss);
+/* Adam (beta 0.9 / 0.999) over seeded random batches of the training set; *final_loss = mean loss of the last
+ * tenth of the steps, *gpu_ms = device time of the training */
+ifea_status ifea_mlp_train(ifea_mlp *m, int32_t steps, int32_t batch, float lr, uint64_t seed, float *final_loss,
+                           double *gpu_ms);
+/* mode 0 off; bit 1: record (inputs, target) of every accepted increment into m's training set; bit 2: start
+ * each increment from the network's prediction when the functional is lower there than at the reference's start
+ * (which is kept otherwise). m must outlive the context's use of it. */
+ifea_status ifea3d_set_warm_start(ifea3d *ctx, ifea_mlp *m, int32_t mode);
+
 /* ------------------------------------------------------------------ 2D (ForgingSolver) */
 
 /* SimulationConfig + DieSet fields the 2D path reads (Simulation/SimulationConfig.cs:14-45, Geometry/DieSet.cs). */

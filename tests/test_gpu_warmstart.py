@@ -1,0 +1,152 @@
+"""The learned warm start on the GPU: its tensor-core network against the CPU FP64 network (oracle/mlp_ref.py),
+its training, and what the trained network gains inside the 3D stepper over the reference's start.
+
+Tolerances: against the CPU network that rounds to bfloat16 where the GPU stores bfloat16, only FP32
+accumulation order differs (2e-3 relative in outputs and gradients); against the exact FP64 network the
+bfloat16 storage itself shows (3e-2 relative, gradients' cosine above 0.999).
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import mlp_ref
+from impressionfea_b200.forging3d import Forging3DSolver
+from impressionfea_b200.warmstart import WarmStartNetwork
+from impressionfea_b200.workloads import closed_die_gear_blank
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, float) - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _random_params(seed):
+    rng = np.random.default_rng(seed)
+    p = np.zeros(mlp_ref.NPAR)
+    k = 0
+    for name, shape in mlp_ref.SHAPES:
+        n = int(np.prod(shape))
+        fan_in = shape[1] if len(shape) == 2 else 1
+        p[k:k + n] = rng.uniform(-1, 1, n) * (np.sqrt(3.0 / fan_in) if len(shape) == 2 else 0.2)
+        k += n
+    return p.astype(np.float32)
+
+
+def _net(seed=1, params=None):
+    net = WarmStartNetwork(seed)
+    net.identity_normalisation()
+    if params is not None:
+        net.set_params(params)
+    return net
+
+
+def test_forward_matches_the_cpu_network():
+    rng = np.random.default_rng(7)
+    p = _random_params(1)
+    net = _net(params=p)
+    x = rng.standard_normal((1000, mlp_ref.NIN)).astype(np.float32)  # 1000 rows: a partial last 128-row tile
+    y = net.forward(x)
+    y_bf, _ = mlp_ref.forward(p.astype(np.float64), x.astype(np.float64), bf16=True)
+    y64, _ = mlp_ref.forward(p.astype(np.float64), x.astype(np.float64), bf16=False)
+    assert _rel(y, y_bf) < 2e-3
+    assert _rel(y, y64) < 3e-2
+    net.close()
+
+
+def test_gradients_match_the_cpu_network():
+    rng = np.random.default_rng(8)
+    p = _random_params(2)
+    net = _net(params=p)
+    x = rng.standard_normal((1024, mlp_ref.NIN)).astype(np.float32)
+    t = rng.standard_normal((1024, mlp_ref.NOUT)).astype(np.float32)
+    loss, g = net.gradients(x, t)
+    loss_bf, g_bf = mlp_ref.loss_and_gradients(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64), bf16=True)
+    loss64, g64 = mlp_ref.loss_and_gradients(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64))
+    assert abs(loss / loss_bf - 1) < 1e-3
+    k = 0
+    for name, shape in mlp_ref.SHAPES:
+        n = int(np.prod(shape))
+        a, b, c = g[k:k + n], g_bf[k:k + n], g64[k:k + n]
+        k += n
+        assert _rel(a, b) < 2e-3, f"{name}: {_rel(a, b):.2e} against the bfloat16-rounded CPU network"
+        assert _rel(a, c) < 3e-2, f"{name}: {_rel(a, c):.2e} against the FP64 CPU network"
+        assert float(a @ c) / (np.linalg.norm(a) * np.linalg.norm(c)) > 0.999, name
+    net.close()
+
+
+def test_adam_step_matches_the_cpu_rule():
+    rng = np.random.default_rng(9)
+    p = _random_params(3)
+    net = _net(params=p)
+    x = rng.standard_normal((1024, mlp_ref.NIN)).astype(np.float32)
+    t = rng.standard_normal((1024, mlp_ref.NOUT)).astype(np.float32)
+    _, g = net.gradients(x, t)
+    net.add_samples(x, t)
+    net.train(steps=1, batch=1024, lr=1e-3, seed=5)  # one batch = the whole set, in another order
+    w1, _, _ = mlp_ref.adam_step(p, g, np.zeros_like(p), np.zeros_like(p), 1, 1e-3)
+    big = np.abs(g) > 1e-6  # where the gradient is not at rounding level, the first step is lr * sign(g)
+    np.testing.assert_allclose(net.params()[big], w1[big], rtol=0, atol=1e-6)
+    net.close()
+
+
+def test_training_fits_a_smooth_map():
+    rng = np.random.default_rng(10)
+    x = rng.standard_normal((40000, mlp_ref.NIN)).astype(np.float32)
+    a = rng.standard_normal((mlp_ref.NIN, mlp_ref.NOUT)) / 4
+    t = (np.sin(x @ a) + 0.5 * np.tanh(x[:, :3])).astype(np.float32)
+    net = WarmStartNetwork(4)
+    net.add_samples(x, t)
+    net.fit_normalisation()
+    first = net.train(steps=10, batch=4096, lr=2e-3, seed=1)
+    last = net.train(steps=400, batch=4096, lr=2e-3, seed=2)
+    assert last < 0.05 < first, f"normalised loss {first:.3f} -> {last:.4f}"
+    y = net.forward(x[:2000])
+    assert _rel(y, t[:2000]) < 0.15
+    net.close()
+
+
+def _small_gear_blank(seed):
+    cfg, mesh, dies = closed_die_gear_blank(target_tets=20000, seed=seed)
+    return cfg, mesh, dies
+
+
+def _run(cfg, mesh, dies, increments, net=None, record=False, predict=False):
+    s = Forging3DSolver(cfg, mesh, dies)
+    s.set_scalar("factor_fp32", 1)
+    if net is not None:
+        net.attach(s, record=record, predict=predict)
+    its, facts, loads = 0, 0, []
+    for _ in range(increments):
+        info = s.step()
+        its += info["iterations"]
+        loads.append(info["load"])
+    facts = int(s.scalar("n_fact"))
+    used, fallbacks = s.scalar("ws_used"), s.scalar("ws_fallbacks")
+    s.close()
+    return its, facts, np.array(loads), used, fallbacks
+
+
+def test_trained_start_against_the_reference_start_on_a_closed_die():
+    # trajectories of two seeded variants of the gear-blank case train the network; a third variant is then run
+    # from the reference's start and from the network's start, over the same increments
+    net = WarmStartNetwork(11)
+    for seed in (21, 22):
+        cfg, mesh, dies = _small_gear_blank(seed)
+        _run(cfg, mesh, dies, 14, net, record=True)
+    n_samples = net.samples
+    assert n_samples > 100000
+    net.fit_normalisation()
+    loss = net.train(steps=800, batch=8192, lr=1e-3, seed=3)
+    cfg, mesh, dies = _small_gear_blank(23)
+    it_ref, f_ref, load_ref, _, _ = _run(cfg, mesh, dies, 14)
+    it_net, f_net, load_net, used, fallbacks = _run(cfg, mesh, dies, 14, net, predict=True)
+    load_err = float(np.max(np.abs(load_net / load_ref - 1)))
+    report = (f"samples {n_samples}, loss {loss:.4f}, Newton iterations {it_ref} -> {it_net}, factorisations "
+              f"{f_ref} -> {f_net}, network start used {used:.0f} / fallback {fallbacks:.0f}, load diff {load_err:.2e}")
+    print(report)
+    assert load_err < 5e-3, report
+    assert used > 0, report
+    assert it_net <= it_ref, report
+    net.close()
