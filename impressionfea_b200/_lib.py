@@ -64,6 +64,8 @@ class StepInfo(C.Structure):
 _vp, _dp, _i32p, _u8p, _i64p = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_uint8), C.POINTER(C.c_int64)
 _st = C.c_int
 _fp = C.POINTER(C.c_float)
+INSIDE_FN = C.CFUNCTYPE(C.c_int32, C.c_double, C.c_double, C.c_double, C.c_void_p)
+SIZE_FN = C.CFUNCTYPE(C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p)
 
 SIGNATURES = {
     "ifea3d_create": (_st, [C.POINTER(Params3D), C.POINTER(_vp)]),
@@ -125,6 +127,13 @@ SIGNATURES = {
     "ifea_mlp_gradients": (_st, [_vp, _fp, _fp, C.c_int64, _fp, _fp]),
     "ifea_mlp_train": (_st, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _fp, _dp]),
     "ifea3d_set_warm_start": (_st, [_vp, _vp, C.c_int32]),
+    "ifea3d_last_remesh": (C.c_char_p, [_vp]),
+    "ifea_tetmesh_stuff": (_st, [INSIDE_FN, _vp, _dp, _dp, C.c_double, C.c_int32, C.c_int32, C.POINTER(_vp)]),
+    "ifea_tetmesh_refine": (_st, [_vp, SIZE_FN, _vp, C.c_int32, _i32p]),
+    "ifea_tetmesh_node_count": (C.c_int32, [_vp]),
+    "ifea_tetmesh_tet_count": (C.c_int32, [_vp]),
+    "ifea_tetmesh_get": (_st, [_vp, _dp, _i32p]),
+    "ifea_tetmesh_destroy": (None, [_vp]),
 }
 
 _LIB = None

@@ -430,6 +430,7 @@ WarmStartNet::WarmStartNet(uint64_t seed)
     par_.resize(NPAR); grad_.resize(NPAR); m_.resize(NPAR); v_.resize(NPAR); norm_.resize(NNORM);
     w1_.resize(HID * NIN); w2_.resize(HID * HID); w3_.resize(HID * HID); w2t_.resize(HID * HID); w3t_.resize(HID * HID);
     loss_.resize(4);
+    loss_.zero(st_);  // slots 2-3 are the tensor-core error flag and its copy: they must start at zero
     hloss_.resize(4);
     // He-uniform initial weights, zero biases (seeded)
     std::vector<float> p(NPAR, 0.0f);

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "remesh.h"
 #include "warmstart.h"
 #include "kernels3d.cuh"
 #include "mesh3d.h"
@@ -105,6 +106,12 @@ __global__ void k_ws_guess(View3 V, const double *__restrict__ v0, const float *
     }
 }
 
+// out = a + s (b - a), elementwise
+__global__ void k_ws_mix(int n, const double *__restrict__ a, const double *__restrict__ b, double s, double *__restrict__ out)
+{
+    GRID_STRIDE(i, n) { out[i] = a[i] + s * (b[i] - a[i]); }
+}
+
 struct PhaseTimer {
     double &acc;
     std::chrono::steady_clock::time_point t0;
@@ -153,10 +160,24 @@ struct Forging3D {
     // learned warm start: mode bit 1 records (inputs, target) of every accepted increment into the network's
     // training set, bit 2 starts each increment from the network's prediction when its energy is lower than
     // the reference start's (else the reference start is kept)
+    // remeshing (RemeshCore, Forging3DSolver.cs:1958-2101) on the host where the reference remeshes; off by
+    // default, so that increments stay comparable with the oracle, which counts the requests instead
+    bool remesh_enabled = false;
+    int remesh_count = 0, remesh_rejected = 0, refinement_levels = 1, max_nodes = 1 << 30;
+    double t_remesh = 0;
+    std::vector<HotSpot> hot;        // places where increments failed (later remeshes refine there)
+    d3 fail_at = mk3(0, 0, 0);
+    bool have_fail_at = false;
+    std::vector<double> die_host[2];  // host copies of the die heights (the remesher's clearances)
+    std::string last_remesh;
     WarmStartNet *ws_net = nullptr;
     int ws_mode = 0, ws_used = 0, ws_fallbacks = 0;
+    // 0: the lower-functional start of the two; 1: the network's start always; 2: a step along the prediction
+    // from the reference start, chosen on the functional (the reference start when no step lowers it)
+    int ws_policy = 2;
+    double ws_last_step = 0;
     DBuf<float> d_wsf, d_wst, d_wsy;
-    DBuf<double> d_wsv0;
+    DBuf<double> d_wsv0, d_wstry;
     int pcg_failures = 0, pcg_skip = 0, pcg_failures_total = 0;
     // mesh
     TetTopology topo;
@@ -414,6 +435,7 @@ struct Forging3D {
     {
         if (side < 0 || side > 1 || nx < 1 || ny < 1 || !(dx > 0)) throw Failure(IFEA_INPUT_INVALID, "invalid die grid");
         die_h[side].upload(hh, (size_t)(nx + 1) * (ny + 1), st);
+        die_host[side].assign(hh, hh + (size_t)(nx + 1) * (ny + 1));
         die[side].side = side; die[side].nx = nx; die[side].ny = ny;
         die[side].x0 = x0; die[side].y0 = y0; die[side].dx = dx; die[side].h = die_h[side].p;
         have_dies |= 1 << side;
@@ -494,16 +516,56 @@ struct Forging3D {
         if (!(ws_mode & 2) || !warm || !have_vg_prev) return;
         d_wsy.resize((size_t)3 * nn);
         ws_net->infer_device(d_wsf, nn, d_wsy, st);
-        // keep whichever start has the lower value of the functional (the Newton iteration minimises it)
-        double e_ref = assemble(ASM_ENERGY, 0, d_vbuf[vcur], false, nullptr);
         k_ws_guess<<<grid(nn), 256, 0, st>>>(V, d_wsv0, d_wsy, d_vbuf[1 - vcur]);
-        double e_net = assemble(ASM_ENERGY, 0, d_vbuf[1 - vcur], false, nullptr);
-        if (e_net < e_ref) {
+        if (ws_policy == 1) {  // the network's start, unconditionally
             vcur = 1 - vcur;
             ws_used++;
-        } else {
-            ws_fallbacks++;
+            return;
         }
+        // the Newton iteration minimises the functional: measure the starts by it
+        double e_ref = assemble(ASM_ENERGY, 0, d_vbuf[vcur], false, nullptr);
+        double e_net = assemble(ASM_ENERGY, 0, d_vbuf[1 - vcur], false, nullptr);
+        if (ws_policy == 0) {  // whichever start has the lower value
+            if (e_net < e_ref) {
+                vcur = 1 - vcur;
+                ws_used++;
+            } else {
+                ws_fallbacks++;
+            }
+            return;
+        }
+        // policy 2: the prediction as a search direction from the reference start, v(a) = v_ref + a (v_net - v_ref),
+        // with the step from a parabola through a = 0, 1/2, 1 (clamped to [0, 1.5]); the lowest of the tried
+        // points is kept, so the reference start (a = 0) stays the fallback
+        int n = topo.ndof;
+        d_wstry.resize((size_t)n);
+        const double *v0 = d_vbuf[vcur], *v1 = d_vbuf[1 - vcur];
+        k_ws_mix<<<grid(n), 256, 0, st>>>(n, v0, v1, 0.5, d_wstry);
+        double e_half = assemble(ASM_ENERGY, 0, d_wstry, false, nullptr);
+        double c2 = 2 * (e_ref - 2 * e_half + e_net), c1 = e_net - e_ref - c2;  // e(a) = e_ref + c1 a + c2 a^2
+        double best_a = 0, best_e = e_ref;
+        if (e_half < best_e) { best_a = 0.5; best_e = e_half; }
+        if (e_net < best_e) { best_a = 1.0; best_e = e_net; }
+        if (c2 > 0) {
+            double a = rclamp(-c1 / (2 * c2), 0.0, 1.5);
+            if (a != 0 && a != 0.5 && a != 1.0) {
+                k_ws_mix<<<grid(n), 256, 0, st>>>(n, v0, v1, a, d_wstry);
+                double e_a = assemble(ASM_ENERGY, 0, d_wstry, false, nullptr);
+                if (e_a < best_e) { best_a = a; best_e = e_a; }
+            }
+        }
+        ws_last_step = best_a;
+        if (best_a == 0) {
+            ws_fallbacks++;
+            return;
+        }
+        ws_used++;
+        if (best_a == 1.0) {
+            vcur = 1 - vcur;
+            return;
+        }
+        k_ws_mix<<<grid(n), 256, 0, st>>>(n, v0, v1, best_a, d_vbuf[1 - vcur]);
+        vcur = 1 - vcur;
     }
 
     void warm_start_record()
@@ -801,12 +863,73 @@ struct Forging3D {
         read_err(e4);
         if (e4[1] != INT_MAX) {
             why = fmt("tetrahedron %d collapsed", e4[1]);
+            {
+                // the failure point for local refinement at the next remesh: the collapsed tet's centroid
+                double xt[12];
+                for (int a = 0; a < 4; a++)
+                    cuda_check(cudaMemcpyAsync(xt + 3 * a, d_xT.p + 3 * (size_t)topo.tets[4 * (size_t)e4[1] + a],
+                                               3 * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+                cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+                fail_at = mk3(0.25 * (xt[0] + xt[3] + xt[6] + xt[9]), 0.25 * (xt[1] + xt[4] + xt[7] + xt[10]),
+                              0.25 * (xt[2] + xt[5] + xt[8] + xt[11]));
+                have_fail_at = true;
+            }
             return false;
         }
         std::swap(d_x.p, d_xT.p);
         std::swap(d_contact.p, d_cT.p);
         gap = gapT;
         time += dt;
+        return true;
+    }
+
+    // ---------------------------------------------------------------- Remesh (:1945-2101)
+    bool remesh(const std::string &reason)
+    {
+        PhaseTimer pt(t_remesh);
+        if (die_host[0].empty() || die_host[1].empty()) throw Failure(IFEA_BAD_STATE, "remeshing needs both dies");
+        size_t nn = topo.nn, ne = topo.ne;
+        std::vector<double> x(3 * nn), vg(3 * nn), eps(ne), dmg(ne), sig(ne), rate(ne), mean(ne);
+        d_x.download(x.data(), 3 * nn, st);
+        d_vg.download(vg.data(), 3 * nn, st);
+        d_eps.download(eps.data(), ne, st);
+        d_dmg.download(dmg.data(), ne, st);
+        d_elsig.download(sig.data(), ne, st);
+        d_elrate.download(rate.data(), ne, st);
+        d_elmean.download(mean.data(), ne, st);
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        RemeshInput in;
+        in.nn = (int)nn; in.ne = (int)ne; in.x = x.data(); in.tets = topo.tets.data(); in.vg = vg.data();
+        in.eps = eps.data(); in.dmg = dmg.data(); in.sig = sig.data(); in.rate = rate.data(); in.mean = mean.data();
+        for (int k = 0; k < 2; k++) {
+            in.die[k] = die[k];
+            in.die[k].h = die_host[k].data();
+        }
+        in.gap = gap; in.h = h; in.vol_target = vol0 / P.sym_factor; in.sym_x = P.sym_x != 0; in.sym_y = P.sym_y != 0;
+        in.recovery_pass = recovery_pass; in.refinement_levels = refinement_levels; in.max_nodes = max_nodes;
+        in.sig_ref = sig_ref; in.hot = hot;
+        RemeshOutput out;
+        if (!remesh_workpiece(in, out)) {
+            remesh_rejected++;
+            last_remesh = reason + " rejected: " + out.why;
+            return false;
+        }
+        int nn2 = (int)(out.x.size() / 3), ne2 = (int)(out.tets.size() / 4);
+        set_mesh(nn2, ne2, out.x.data(), out.tets.data(), out.on_x0.data(), out.on_y0.data());
+        d_vg.upload(out.vg, st);
+        d_eps.upload(out.eps, st);
+        d_dmg.upload(out.dmg, st);
+        d_elsig.upload(out.sig, st);
+        d_elrate.upload(out.rate, st);
+        d_elmean.upload(out.mean, st);
+        d_contact.upload(out.contact, st);
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        have_vg_prev = false;
+        warm = 0;
+        factor_step = -1;
+        remesh_count++;
+        last_remesh = fmt("%s: q_min %.3f -> %.3f, %d tets, %d nodes, %d local refinements", reason.c_str(), out.q_old,
+                          out.q_new, ne2, nn2, out.splits);
         return true;
     }
 
@@ -821,13 +944,18 @@ struct Forging3D {
         {
             PhaseTimer pt(t_trigger);
             double rq = P.remesh_quality;
+            const char *trigger = nullptr;
             if (min_quality(d_x) < rq) smooth_interior(d_x, rq, 6);
-            if (min_quality(d_x) < rq) remesh_requests++;
+            if (min_quality(d_x) < rq) trigger = "element quality";
             else {
                 View3 V = view();
                 k_edges_layers<<<kReduceBlocks, 256, 0, st>>>(V);
                 finalize({MAXS(S_MAXEDGE), MAXS(S_THIN)});
-                if (read_scalars()[S_MAXEDGE] > 2.8 * h) remesh_requests++;
+                if (read_scalars()[S_MAXEDGE] > 2.8 * h) trigger = "surface stretched";
+            }
+            if (trigger) {
+                remesh_requests++;
+                if (remesh_enabled) remesh(trigger);
             }
         }
         double step_cap = P.ds * h / P.h;
@@ -843,7 +971,10 @@ struct Forging3D {
             its = solve_velocity(&converged, cancel);
             if (!converged) {
                 if (!(last_rel < 1e-2)) {
-                    if (pass < passes - 1) remesh_requests++;
+                    if (pass < passes - 1) {
+                        remesh_requests++;
+                        if (remesh_enabled && remesh("stalled velocity solution")) continue;
+                    }
                     throw Failure(IFEA_DIVERGED, fmt("Velocity solution did not converge at step %d (stroke %.3f mm): |dv|/|v| = %.2e.",
                                                      step_index, gap0 - gap, last_rel));
                 }
@@ -869,7 +1000,13 @@ struct Forging3D {
                 }
             }
             if (ok || pass == passes - 1) break;
-            remesh_requests++;  // Remesh(...) would run here; unavailable, so the ladder continues
+            if (pass >= 1 && refinement_levels > 0 && have_fail_at) {
+                hot.push_back({fail_at, std::min(pass, refinement_levels)});
+                if (hot.size() > 64) hot.erase(hot.begin());
+            }
+            remesh_requests++;
+            // a rejected remesh does not end the ladder: the next pass relaxes the corner tolerance
+            if (remesh_enabled) remesh(pass == 0 ? "fold during update" : "recovery");
         }
         recovery_pass = 0;
         if (!ok)
@@ -952,7 +1089,10 @@ struct Forging3D {
         S("t_graph_solve", lin->setup_s(3)) S("factor_gpu_ms", lin->factor_ms()) S("solve_gpu_ms", lin->solve_ms()) S("solves", lin->solves())
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
         S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows) S("tc_updates", lin->tc_launches())
-        S("ws_used", ws_used) S("ws_fallbacks", ws_fallbacks) S("ws_mode", ws_mode)
+        S("ws_used", ws_used) S("ws_fallbacks", ws_fallbacks) S("ws_mode", ws_mode) S("ws_policy", ws_policy)
+        S("ws_last_step", ws_last_step)
+        S("remesh", remesh_enabled) S("remesh_count", remesh_count) S("remesh_rejected", remesh_rejected)
+        S("t_remesh", t_remesh) S("refinement_levels", refinement_levels) S("max_nodes", max_nodes) S("hot_spots", hot.size())
 #undef S
         if (nm == "volume") return volume();
         if (nm == "min_quality") return min_quality(d_x);
@@ -976,6 +1116,15 @@ struct Forging3D {
             use_precision(v != 0);
             pcg_early_abort = v != 0;
         } else if (nm == "pcg_early_abort") pcg_early_abort = v != 0;
+        else if (nm == "remesh") remesh_enabled = v != 0;
+        else if (nm == "ws_policy") {
+            if (v != 0 && v != 1 && v != 2) throw Failure(IFEA_INPUT_INVALID, "ws_policy: 0, 1 or 2");
+            ws_policy = (int)v;
+        }
+        else if (nm == "refinement_levels") {
+            if (v < 0 || v > 3) throw Failure(IFEA_INPUT_INVALID, "Refinement levels must be 0-3.");
+            refinement_levels = (int)v;
+        } else if (nm == "max_nodes") max_nodes = (int)v;
         else if (nm == "ordering") {
             if (v != 0 && v != 1) throw Failure(IFEA_INPUT_INVALID, "ordering: 0 (METIS) or 1 (coordinate nested dissection)");
             if ((int)v != ordering) {
@@ -1145,6 +1294,8 @@ ifea_status ifea3d_set_stream(ifea3d *ctx, void *cuda_stream)
 {
     return guarded(ctx, [&](Forging3D &s) { s.set_stream((cudaStream_t)cuda_stream); });
 }
+
+const char *ifea3d_last_remesh(const ifea3d *ctx) { return ctx && ctx->s ? ctx->s->last_remesh.c_str() : ""; }
 
 ifea_status ifea3d_set_warm_start(ifea3d *ctx, ifea_mlp *mlp, int32_t mode)
 {

@@ -151,6 +151,29 @@ ifea_status ifea_spd_solve(ifea_spd *s, const double *b, double *x);
 int64_t ifea_spd_factor_nonzeros(const ifea_spd *s);
 const char *ifea_spd_name(const ifea_spd *s);
 
+/* ------------------------------------------------------------------ remeshing (3D, host side)
+ *
+ * With ifea3d_set_scalar(ctx, "remesh", 1) the stepper remeshes where the reference does (RemeshTrigger at the
+ * start of an increment, a stalled velocity solution, a fold during the update: ThreeD/Forging3DSolver.cs:544-611)
+ * by RemeshCore (:1958-2101) on the host and continues on the new mesh with the remapped state; off by default
+ * (the requests are only counted). "refinement_levels" (0-3, default 1) and "max_nodes" bound the local
+ * refinement around failures. The two building blocks are exported as the reference's public statics: */
+typedef int32_t (*ifea_inside_fn)(double x, double y, double z, void *user);
+typedef double (*ifea_size_fn)(double x, double y, double z, void *user);
+typedef struct ifea_tetmesh ifea_tetmesh;
+/* IsosurfaceStuffing.Stuff (ThreeD/IsosurfaceStuffing.cs:19-84): body-centred-cubic lattice of spacing h over
+ * [lo, hi], cut, warped and clipped to the body; sym_x / sym_y keep x >= 0 / y >= 0 with flat symmetry planes */
+ifea_status ifea_tetmesh_stuff(ifea_inside_fn inside, void *user, const double *lo3, const double *hi3, double h,
+                               int32_t sym_x, int32_t sym_y, ifea_tetmesh **out);
+/* TetRefiner.Refine (ThreeD/TetRefiner.cs:14-158): longest-edge bisection to the target size, within max_nodes */
+ifea_status ifea_tetmesh_refine(ifea_tetmesh *m, ifea_size_fn size, void *user, int32_t max_nodes, int32_t *splits);
+int32_t ifea_tetmesh_node_count(const ifea_tetmesh *m);
+int32_t ifea_tetmesh_tet_count(const ifea_tetmesh *m);
+ifea_status ifea_tetmesh_get(const ifea_tetmesh *m, double *x, int32_t *tets);
+void ifea_tetmesh_destroy(ifea_tetmesh *m);
+/* why the last remesh of the context was rejected, or what the last accepted one made */
+const char *ifea3d_last_remesh(const ifea3d *ctx);
+
 /* ------------------------------------------------------------------ learned warm start (3D)
  *
  * Replaces the initial velocity guess of each increment, LoadVelocityGuess (ThreeD/Forging3DSolver.cs:854-869:

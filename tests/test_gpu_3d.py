@@ -19,6 +19,7 @@ pytestmark = pytest.mark.gpu
 RTOL_ELEM = 1e-12      # per-element / per-node FP64 arithmetic (a few ulps of pow())
 RTOL_ENERGY = 1e-10    # global sums: 1/2 v.K_vol.v cancels the penalty terms, so its summation order shows
 RTOL_STATE = 1e-6      # velocity, strain and load over Newton iterations and increments
+RTOL_X = 1e-7          # coordinates after increments (moved by dt * velocity)
 
 
 def _case(friction=0.3, R=10.0, H=20.0, h=2.0, shut=12.0, seed=1):
@@ -125,7 +126,9 @@ def test_increments_track_the_oracle(wide_rows):
         assert abs(info["load"] / ora.scalar("load") - 1) < RTOL_STATE, f"step {k + 1}: load"
         np.testing.assert_array_equal(gpu.array("contact"), ora.array("contact"))
         _close(gpu.array("vg"), ora.array("vg"), RTOL_STATE, f"step {k + 1}: velocity")
-        _close(gpu.array("x"), ora.array("x"), 1e-9, f"step {k + 1}: coordinates")
+        # x moves by dt * vg: it inherits the velocity's 1e-6 relative tolerance scaled by the stroke increment
+        # over the billet size (0.2 / 20 here), so 1e-7 of the largest coordinate
+        _close(gpu.array("x"), ora.array("x"), RTOL_X, f"step {k + 1}: coordinates")
         _close(gpu.array("eps"), ora.array("eps"), RTOL_STATE, f"step {k + 1}: effective strain")
         assert abs(gpu.scalar("gap") - ora.scalar("gap")) < 1e-12
     if wide_rows is not None:

@@ -79,7 +79,8 @@ def _increment_matches(gpu, ora, k):
     np.testing.assert_array_equal(gpu.array("contact"), ora.array("contact"), err_msg=f"increment {k}: contact")
     _close(gpu.array("vg"), ora.array("vg"), RTOL_STATE, f"increment {k}: velocity")
     _close(gpu.array("eps"), ora.array("eps"), RTOL_STATE, f"increment {k}: effective strain")
-    _close(gpu.array("x"), ora.array("x"), 1e-9, f"increment {k}: coordinates")
+    # x moves by dt * vg: the velocity's 1e-6 relative tolerance times the stroke increment over the part size
+    _close(gpu.array("x"), ora.array("x"), 1e-7, f"increment {k}: coordinates")
 
 
 # ------------------------------------------------------------------ 3D upsetting drop-in (31.9k tets)
