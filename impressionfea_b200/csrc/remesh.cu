@@ -11,9 +11,11 @@
 #include "remesh.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <thread>
 #include <unordered_map>
 #include <utility>
 
@@ -22,6 +24,25 @@
 namespace ifea {
 
 namespace {
+
+// f(i) for i in [0, n) on the host's threads (contiguous chunks); serial for small n
+template <class F>
+void parallel_for(int n, F &&f, bool parallel = true)
+{
+    int nt = parallel && n >= 4096 ? (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    if (nt == 1) {
+        for (int i = 0; i < n; i++) f(i);
+        return;
+    }
+    int chunk = (n + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; t++)
+        th.emplace_back([&, t] {
+            int a = t * chunk, b = std::min(n, a + chunk);
+            for (int i = a; i < b; i++) f(i);
+        });
+    for (auto &x : th) x.join();
+}
 
 inline uint64_t edge_key(int a, int b)
 {
@@ -146,6 +167,16 @@ TetLocator::TetLocator(const std::vector<d3> &x, const std::vector<int32_t> &tet
     items_.assign(start_[ncell], 0);
     std::vector<int32_t> fill(start_.begin(), start_.end() - 1);
     for (int e = 0; e < ne; e++) each(e, [&](size_t c) { items_[fill[c]++] = e; });
+    nstart_.assign(ncell + 1, 0);
+    std::vector<int32_t> ncell_of(x.size());
+    for (size_t n = 0; n < x.size(); n++) {
+        ncell_of[n] = cell_of(x[n]);
+        nstart_[ncell_of[n] + 1]++;
+    }
+    for (size_t c = 0; c < ncell; c++) nstart_[c + 1] += nstart_[c];
+    nitems_.assign(x.size(), 0);
+    std::vector<int32_t> nfill(nstart_.begin(), nstart_.end() - 1);
+    for (size_t n = 0; n < x.size(); n++) nitems_[nfill[ncell_of[n]]++] = (int32_t)n;
 }
 
 int TetLocator::cell_of(d3 p) const
@@ -184,16 +215,38 @@ d3 TetLocator::interpolate(d3 p, const double *field) const
         for (int a = 1; a < 4; a++) r = add3(r, scl3(w[a], ld3(field, t_[4 * e + a])));
         return r;
     }
-    int best = 0;
+    return ld3(field, nearest_node(p));
+}
+
+// the nearest node (the lowest index among equally near ones), searched ring by ring over a grid of nodes; any
+// node outside the rings searched so far is at least r cells away
+int TetLocator::nearest_node(d3 p) const
+{
+    int ci = iclamp((int)((p.x - min_.x) / cell_), 0, nx_ - 1), cj = iclamp((int)((p.y - min_.y) / cell_), 0, ny_ - 1),
+        ck = iclamp((int)((p.z - min_.z) / cell_), 0, nz_ - 1);
     double dmin = DBL_MAX;
-    for (size_t n = 0; n < x_.size(); n++) {
-        double dd = len23(sub3(x_[n], p));
-        if (dd < dmin) {
-            dmin = dd;
-            best = (int)n;
-        }
+    int best = 0;
+    int rmax = std::max(nx_, std::max(ny_, nz_));
+    for (int r = 0; r <= rmax; r++) {
+        for (int k = ck - r; k <= ck + r; k++)
+            for (int j = cj - r; j <= cj + r; j++)
+                for (int i = ci - r; i <= ci + r; i++) {
+                    if (i < 0 || j < 0 || k < 0 || i >= nx_ || j >= ny_ || k >= nz_) continue;
+                    if (std::max(std::abs(i - ci), std::max(std::abs(j - cj), std::abs(k - ck))) != r) continue;
+                    size_t c = ((size_t)k * ny_ + j) * nx_ + i;
+                    for (int32_t q = nstart_[c]; q < nstart_[c + 1]; q++) {
+                        int n = nitems_[q];
+                        double dd = len23(sub3(x_[n], p));
+                        if (dd < dmin || (dd == dmin && n < best)) {
+                            dmin = dd;
+                            best = n;
+                        }
+                    }
+                }
+        // a point outside the grid box is farther still from everything beyond ring r, so this stop is safe
+        if (dmin < DBL_MAX && sqrt(dmin) <= r * cell_) break;
     }
-    return ld3(field, best);
+    return best;
 }
 
 int TetLocator::find_nearest(d3 p) const
@@ -225,7 +278,7 @@ int TetLocator::find_nearest(d3 p) const
 // ------------------------------------------------------------------ isosurface stuffing (ThreeD/IsosurfaceStuffing.cs)
 
 void stuff_uniform(const std::function<bool(d3)> &inside, d3 lo, d3 hi, double h, bool sym_x, bool sym_y,
-                   std::vector<d3> &out_pts, std::vector<int32_t> &out_tets)
+                   std::vector<d3> &out_pts, std::vector<int32_t> &out_tets, bool parallel)
 {
     const double alpha_long = 0.24999, alpha_short = 0.41189;  // the published warp thresholds
     const double eps = 1e-7 * h;
@@ -269,10 +322,11 @@ void stuff_uniform(const std::function<bool(d3)> &inside, d3 lo, d3 hi, double h
             }
     auto is_corner = [&](int v) { return v < n_corner; };
     std::vector<int8_t> sign(pos.size());
-    for (size_t v = 0; v < pos.size(); v++) sign[v] = In(pos[v]) ? -1 : 1;
+    parallel_for((int)pos.size(), [&](int v) { sign[v] = In(pos[v]) ? -1 : 1; }, parallel);
     auto crosses = [&](int u, int w) { return (sign[u] < 0 && sign[w] > 0) || (sign[u] > 0 && sign[w] < 0); };
     const int ea[6] = {0, 0, 0, 1, 1, 2}, eb[6] = {1, 2, 3, 2, 3, 3};
-    // cut points on the edges between an inside and an outside vertex, bisected on the inside test, in creation order
+    // cut points on the edges between an inside and an outside vertex, in creation order, each bisected on the
+    // inside test (independently of the others)
     std::unordered_map<uint64_t, int> cut_index;
     std::vector<std::pair<uint64_t, d3>> cuts;
     for (size_t t = 0; t < lat.size(); t += 4)
@@ -281,18 +335,22 @@ void stuff_uniform(const std::function<bool(d3)> &inside, d3 lo, d3 hi, double h
             if (!crosses(u, w)) continue;
             uint64_t key = edge_key(u, w);
             if (cut_index.count(key)) continue;
-            d3 pin = sign[u] < 0 ? pos[u] : pos[w], pout = sign[u] < 0 ? pos[w] : pos[u];
-            for (int it = 0; it < 16; it++) {
-                d3 m = scl3(0.5, add3(pin, pout));
-                if (In(m)) pin = m;
-                else pout = m;
-            }
-            d3 cp = scl3(0.5, add3(pin, pout));
-            if (sym_x && fabs(cp.x) < 1e-4 * h) cp.x = 0;
-            if (sym_y && fabs(cp.y) < 1e-4 * h) cp.y = 0;
             cut_index[key] = (int)cuts.size();
-            cuts.push_back({key, cp});
+            cuts.push_back({key, mk3(0, 0, 0)});
         }
+    parallel_for((int)cuts.size(), [&](int ci) {
+        int u = (int)(cuts[ci].first >> 32), w = (int)(cuts[ci].first & 0xffffffffu);
+        d3 pin = sign[u] < 0 ? pos[u] : pos[w], pout = sign[u] < 0 ? pos[w] : pos[u];
+        for (int it = 0; it < 16; it++) {
+            d3 m = scl3(0.5, add3(pin, pout));
+            if (In(m)) pin = m;
+            else pout = m;
+        }
+        d3 cp = scl3(0.5, add3(pin, pout));
+        if (sym_x && fabs(cp.x) < 1e-4 * h) cp.x = 0;
+        if (sym_y && fabs(cp.y) < 1e-4 * h) cp.y = 0;
+        cuts[ci].second = cp;
+    }, parallel);
     // warp lattice vertices too close to a cut point onto it (the nearest cut; the first on ties)
     std::vector<int> warp_to(pos.size(), -1);
     std::vector<double> warp_d(pos.size(), DBL_MAX);
@@ -420,9 +478,22 @@ void stuff_uniform(const std::function<bool(d3)> &inside, d3 lo, d3 hi, double h
 
 // ------------------------------------------------------------------ local refinement (ThreeD/TetRefiner.cs)
 
+namespace {
+struct EdgeHash {
+    size_t operator()(uint64_t k) const
+    {
+        k ^= k >> 33;
+        k *= 0xff51afd7ed558ccdULL;
+        k ^= k >> 33;
+        return (size_t)k;
+    }
+};
+}  // namespace
+
 int refine_tets(std::vector<d3> &pts, std::vector<int32_t> &tl, const std::function<double(d3)> &target, int max_nodes)
 {
-    std::unordered_map<uint64_t, std::vector<int>> edges;
+    std::unordered_map<uint64_t, std::vector<int>, EdgeHash> edges;
+    edges.reserve(tl.size() * 2);
     auto add_edges = [&](int e) {
         for (int i = 0; i < 4; i++)
             for (int j = i + 1; j < 4; j++) edges[edge_key(tl[4 * (size_t)e + i], tl[4 * (size_t)e + j])].push_back(e);
@@ -498,6 +569,14 @@ int refine_tets(std::vector<d3> &pts, std::vector<int32_t> &tl, const std::funct
         }
         return count;
     };
+    // the edge map is built only when some tet needs refining
+    bool any = false;
+    for (int e = 0; e < (int)(tl.size() / 4) && !any; e++) {
+        int a, b;
+        double len = longest(e, a, b);
+        any = len > 1.05 * target(centroid4(pts, tl.data() + 4 * (size_t)e));
+    }
+    if (!any) return 0;
     for (int e = 0; e < (int)(tl.size() / 4); e++) add_edges(e);
     int splits = 0;
     for (int pass = 0; pass < 12 && (int)pts.size() < max_nodes; pass++) {
@@ -812,8 +891,16 @@ void compensate_volume(const RemeshInput &in, const LightMesh &M, const std::vec
 
 }  // namespace
 
+namespace {
+double seconds_since(std::chrono::steady_clock::time_point t0)
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+}  // namespace
+
 bool remesh_workpiece(const RemeshInput &in, RemeshOutput &out)
 {
+    auto t0 = std::chrono::steady_clock::now();
     std::vector<d3> ox(in.nn);
     for (int n = 0; n < in.nn; n++) ox[n] = ld3(in.x, n);
     std::vector<int32_t> ot(in.tets, in.tets + 4 * (size_t)in.ne);
@@ -826,11 +913,13 @@ bool remesh_workpiece(const RemeshInput &in, RemeshOutput &out)
     }
     std::vector<d3> x;
     std::vector<int32_t> t;
-    stuff_uniform([&](d3 p) { return locator.contains(p); }, lo, hi, in.h, in.sym_x, in.sym_y, x, t);
+    stuff_uniform([&](d3 p) { return locator.contains(p); }, lo, hi, in.h, in.sym_x, in.sym_y, x, t, true);
     if (t.empty()) {
         out.why = "isosurface stuffing produced no tetrahedra";
         return false;
     }
+    out.t_stuff = seconds_since(t0);
+    t0 = std::chrono::steady_clock::now();
     if (in.refinement_levels > 0) {
         // TargetSize (:287-305) with the reference defaults (no graded mesh, thin-flash or die-edge refinement): h,
         // and h / 2^level within 2 h of the places where earlier increments failed
@@ -843,6 +932,8 @@ bool remesh_workpiece(const RemeshInput &in, RemeshOutput &out)
         };
         out.splits = refine_tets(x, t, target, in.max_nodes);
     }
+    out.t_refine = seconds_since(t0);
+    t0 = std::chrono::steady_clock::now();
     int nn = (int)x.size();
     LightMesh M;
     if (!M.build(nn, t, x, in.sym_x, in.sym_y)) {
@@ -895,25 +986,28 @@ bool remesh_workpiece(const RemeshInput &in, RemeshOutput &out)
         out.why = buf;
         return false;
     }
+    out.t_place = seconds_since(t0);
+    t0 = std::chrono::steady_clock::now();
     int ne = M.ne;
     out.eps.assign(ne, 0); out.dmg.assign(ne, 0); out.sig.assign(ne, in.sig_ref); out.rate.assign(ne, 0); out.mean.assign(ne, 0);
-    for (int e = 0; e < ne; e++) {
+    parallel_for(ne, [&](int e) {
         int f = locator.find_nearest(centroid4(x, t.data() + 4 * (size_t)e));
-        if (f < 0) continue;
+        if (f < 0) return;
         out.eps[e] = in.eps[f];
         out.dmg[e] = in.dmg[f];
         out.sig[e] = in.sig[f];
         out.rate[e] = in.rate[f];
         out.mean[e] = in.mean[f];
-    }
+    });
     out.vg.assign(3 * (size_t)nn, 0);
-    for (int n = 0; n < nn; n++) st3(out.vg.data(), n, locator.interpolate(x[n], in.vg));
+    parallel_for(nn, [&](int n) { st3(out.vg.data(), n, locator.interpolate(x[n], in.vg)); });
     out.x.assign(3 * (size_t)nn, 0);
     for (int n = 0; n < nn; n++) st3(out.x.data(), n, x[n]);
     out.tets = std::move(t);
     out.on_x0 = M.onx;
     out.on_y0 = M.ony;
     out.contact = std::move(contact);
+    out.t_remap = seconds_since(t0);
     return true;
 }
 
@@ -936,7 +1030,7 @@ ifea_status ifea_tetmesh_stuff(ifea_inside_fn inside, void *user, const double *
     try {
         auto *m = new ifea_tetmesh;
         ifea::stuff_uniform([&](d3 p) { return inside(p.x, p.y, p.z, user) != 0; }, mk3(lo3[0], lo3[1], lo3[2]),
-                            mk3(hi3[0], hi3[1], hi3[2]), h, sym_x != 0, sym_y != 0, m->x, m->t);
+                            mk3(hi3[0], hi3[1], hi3[2]), h, sym_x != 0, sym_y != 0, m->x, m->t, false);
         *out = m;
         return IFEA_OK;
     } catch (...) {

@@ -27,6 +27,9 @@ class TetLocator {
     // containing tet, else the tet whose centroid is nearest (first in the point's cell, else over all)
     int find_nearest(d3 p) const;
 
+    // the nearest node (the lowest index among equally near ones)
+    int nearest_node(d3 p) const;
+
   private:
     int cell_of(d3 p) const;
     const std::vector<d3> &x_;
@@ -34,13 +37,14 @@ class TetLocator {
     double cell_;
     d3 min_;
     int nx_, ny_, nz_;
-    std::vector<int32_t> start_, items_;
+    std::vector<int32_t> start_, items_, nstart_, nitems_;
 };
 
 // Isosurface stuffing on the body-centred-cubic lattice of spacing h (IsosurfaceStuffing.Stuff,
 // ThreeD/IsosurfaceStuffing.cs:19-277; Labelle and Shewchuk 2007). Positively oriented tets.
+// With parallel, inside() is called from several host threads at once.
 void stuff_uniform(const std::function<bool(d3)> &inside, d3 lo, d3 hi, double h, bool sym_x, bool sym_y,
-                   std::vector<d3> &pts, std::vector<int32_t> &tets);
+                   std::vector<d3> &pts, std::vector<int32_t> &tets, bool parallel);
 
 // Longest-edge bisection until every tet's longest edge is at most 1.05 target(centroid), within max_nodes
 // (TetRefiner.Refine, ThreeD/TetRefiner.cs:14-158). Returns the number of edge splits.
@@ -73,6 +77,7 @@ struct RemeshOutput {
     double q_old = 0, q_new = 0;
     int splits = 0;
     std::string why;  // the reason a remesh was rejected
+    double t_stuff = 0, t_refine = 0, t_place = 0, t_remap = 0;  // host seconds of the phases
 };
 
 // true: accepted (out holds the new mesh and state); false: rejected, out.why says why

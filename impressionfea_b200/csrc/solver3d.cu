@@ -174,7 +174,7 @@ struct Forging3D {
     int ws_mode = 0, ws_used = 0, ws_fallbacks = 0;
     // 0: the lower-functional start of the two; 1: the network's start always; 2: a step along the prediction
     // from the reference start, chosen on the functional (the reference start when no step lowers it)
-    int ws_policy = 2;
+    int ws_policy = 0;
     double ws_last_step = 0;
     DBuf<float> d_wsf, d_wst, d_wsy;
     DBuf<double> d_wsv0, d_wstry;
@@ -1068,6 +1068,20 @@ struct Forging3D {
         throw Failure(IFEA_INPUT_INVALID, "unknown array name '" + nm + "'");
     }
 
+    // floating-point operations of one factorisation of the current pattern: per front of m rows and k pivot
+    // columns, the lower-triangle updates sum over c < k of (m - c - 1)(m - c) (a multiply and an add each), plus
+    // the pivot column scalings
+    double factor_gflop()
+    {
+        const MfSymbolic &S = lin->symbolic();
+        double f = 0;
+        for (int s = 0; s < S.nsuper; s++) {
+            double m = S.m[s];
+            for (int c = 0; c < S.ncol[s]; c++) f += (m - c - 1) * (m - c) + (m - c - 1);
+        }
+        return f * 1e-9;
+    }
+
     double scalar(const std::string &nm)
     {
 #define S(name, v) if (nm == name) return (double)(v);
@@ -1089,6 +1103,7 @@ struct Forging3D {
         S("t_graph_solve", lin->setup_s(3)) S("factor_gpu_ms", lin->factor_ms()) S("solve_gpu_ms", lin->solve_ms()) S("solves", lin->solves())
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
         S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows) S("tc_updates", lin->tc_launches())
+        S("factor_gflop", factor_gflop())
         S("ws_used", ws_used) S("ws_fallbacks", ws_fallbacks) S("ws_mode", ws_mode) S("ws_policy", ws_policy)
         S("ws_last_step", ws_last_step)
         S("remesh", remesh_enabled) S("remesh_count", remesh_count) S("remesh_rejected", remesh_rejected)

@@ -201,17 +201,32 @@ def gear_blank_thickness(r, hub_r=15.0, hub_t=22.0, web_t=6.0, rim_in=36.0, rim_
     return t
 
 
-def gear_blank_case_3d(h, R=20.0, H=50.0, dx=0.5, seed=0, jitter=0.1, **profile):
+def stuffed_cylinder(R, H, h, z0=0.0):
+    """Quarter-model vertical cylinder (x >= 0, y >= 0) of radius R and height H on z = z0, meshed the way the
+    reference meshes its billets: isosurface stuffing of the solid at lattice spacing h
+    (IsosurfaceStuffing.Stuff, ThreeD/IsosurfaceStuffing.cs:19-84, by the library's host mesher)."""
+    from .remesh import stuff
+
+    x, t = stuff(lambda px, py, pz: px * px + py * py < R * R and z0 < pz < z0 + H, (-R, -R, z0), (R, R, z0 + H), h,
+                 True, True)
+    on_x0 = (x[:, 0] == 0.0).astype(np.uint8)
+    on_y0 = (x[:, 1] == 0.0).astype(np.uint8)
+    return TetCase(x=np.ascontiguousarray(x), tets=np.ascontiguousarray(t, np.int32), on_x0=on_x0, on_y0=on_y0,
+                   gap0=0.0, bounds_for_velocity=(-R, -R, z0, R, R))
+
+
+def gear_blank_case_3d(h, R=20.0, H=50.0, dx=0.5, seed=0, jitter=0.1, stuffed=False, **profile):
     """Closed-die forging of a gear blank (quarter model): billet d = 2R, height H on the bottom die; both dies are
     height fields sampled at dx from gear_blank_thickness, mirrored about the part's mid-plane, the top die given at
     its closed position. The billet seats on the highest point of the bottom die under it (z0 = 0) and the top die
-    starts touching it: gap0 = max over billet nodes of (z - top surface)."""
+    starts touching it: gap0 = max over billet nodes of (z - top surface). stuffed: the billet is meshed by
+    isosurface stuffing at h (as the reference does, and as every remesh does), else by the seeded Delaunay fill."""
     zm = 0.5 * float(np.min(gear_blank_thickness(np.linspace(0.0, R, 401), **profile)))  # seat: z0 = 0
     bottom = HeightField.sample(lambda X, Y: zm - 0.5 * gear_blank_thickness(np.hypot(X, Y), **profile),
                                 -2.0, 70.0, -2.0, 70.0, dx)
     top = HeightField.sample(lambda X, Y: zm + 0.5 * gear_blank_thickness(np.hypot(X, Y), **profile),
                              -2.0, 70.0, -2.0, 70.0, dx)
-    mesh = quarter_cylinder(R, H, h, z0=0.0, seed=seed, jitter=jitter)
+    mesh = stuffed_cylinder(R, H, h) if stuffed else quarter_cylinder(R, H, h, z0=0.0, seed=seed, jitter=jitter)
     r = np.hypot(mesh.x[:, 0], mesh.x[:, 1])
     mesh.gap0 = float(np.max(mesh.x[:, 2] - (zm + 0.5 * gear_blank_thickness(r, **profile))))
     return mesh, (bottom, top)

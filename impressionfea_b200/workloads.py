@@ -4,14 +4,17 @@
   Delaunay fill (node jitter +-10 % of h), flat dies as two-triangle height fields, C = 150 MPa, eps0 = 0.01,
   n = 0.1, m = 0.12, friction m_f = 0.4, 40 % reduction in 80 increments, ram 50 mm/s, tolerance 1e-3.
 - ``closed_die_gear_blank()``: closed-die forging of an axisymmetric gear blank (hub r15, web 6 mm, rim r45,
-  flash gap 3 mm, land 3:1) as two height fields at dx = 0.5 mm, billet d40 x h50, ~205k tets, C = 140 MPa,
-  n = 0.08, m = 0.15, friction 0.3, 200 increments to closure.
+  flash gap 3 mm, land 3:1) as two height fields at dx = 0.5 mm, billet d40 x h50 meshed by isosurface stuffing
+  at 1.0 mm (~202k tets), C = 140 MPa, n = 0.08, m = 0.15, friction 0.3, 200 increments to closure.
 - ``upsetting_2d()``: 2D axisymmetric upsetting, r10 x h30 billet, 20 x 60 quads, flat dies, C = 120 MPa,
   eps0 = 0.01, n = 0.05, m = 0.15, friction 0.3, ram 10 mm/s, 50 % in 100 increments, tolerance 1e-6.
 
-The reference builds its 3D billets by isosurface stuffing (ThreeD/IsosurfaceStuffing.cs); here the same
-generated arrays feed the CUDA path and the oracle, which is all the per-iteration path consumes.
+The reference builds its 3D billets by isosurface stuffing (ThreeD/IsosurfaceStuffing.cs); the closed-die billet
+is stuffed the same way (by the library's host mesher), the upsetting billet is a seeded Delaunay fill. The same
+arrays feed the CUDA path and the oracle, which is all the per-iteration path consumes.
 """
+import numpy as np
+
 from .config import Forging2DConfig, Forging3DConfig
 from .meshes import gear_blank_case_3d, h_for_tets, upset_case_3d
 
@@ -27,11 +30,20 @@ def upsetting_drop_in(target_tets=UPSET_TETS, seed=2024):
     return cfg, mesh, dies
 
 
-def closed_die_gear_blank(target_tets=200000, seed=7):
-    h = round(h_for_tets(20.0, 50.0, target_tets), 3)
-    mesh, dies = gear_blank_case_3d(h, seed=seed, ramp=4.0)
+def closed_die_gear_blank(target_tets=200000, seed=None):
+    """The closed-die case; the billet is meshed by isosurface stuffing, like every remesh after it, at the lattice
+    spacing that gives about target_tets tets (1.0 mm for 200k). seed=None: the published geometry (billet
+    d40 x h50); a seed draws a geometry variant, billet radius and height each within +-5 % (training trajectories
+    for the learned warm start)."""
+    R, H = 20.0, 50.0
+    if seed is not None:
+        rng = np.random.default_rng(seed)
+        R *= rng.uniform(0.95, 1.05)
+        H *= rng.uniform(0.95, 1.05)
+    h = round(1.0 * (200000.0 / target_tets) ** (1.0 / 3.0), 3)
+    mesh, dies = gear_blank_case_3d(h, R=R, H=H, ramp=4.0, stuffed=True)
     cfg = Forging3DConfig(C=140, N=0.08, M=0.15, eps0=0.01, friction=0.3, ram=50.0, h=h, ds=mesh.gap0 / 200,
-                          size=50.0, tol=1e-3)
+                          size=H, tol=1e-3)
     return cfg, mesh, dies
 
 

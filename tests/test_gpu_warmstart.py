@@ -129,16 +129,16 @@ def _run(cfg, mesh, dies, increments, net=None, record=False, predict=False):
 
 
 def test_trained_start_against_the_reference_start_on_a_closed_die():
-    # trajectories of two seeded variants of the gear-blank case train the network; a third variant is then run
+    # trajectories of four seeded variants of the gear-blank case train the network; a fifth variant is then run
     # from the reference's start and from the network's start, over the same increments
     net = WarmStartNetwork(11)
-    for seed in (21, 22):
+    for seed in (21, 22, 24, 25):
         cfg, mesh, dies = _small_gear_blank(seed)
         _run(cfg, mesh, dies, 14, net, record=True)
     n_samples = net.samples
-    assert n_samples > 100000
+    assert n_samples > 200000
     net.fit_normalisation()
-    loss = net.train(steps=800, batch=8192, lr=1e-3, seed=3)
+    loss = net.train(steps=1500, batch=8192, lr=1e-3, seed=3)
     cfg, mesh, dies = _small_gear_blank(23)
     it_ref, f_ref, load_ref, _, _ = _run(cfg, mesh, dies, 14)
     it_net, f_net, load_net, used, fallbacks = _run(cfg, mesh, dies, 14, net, predict=True)
