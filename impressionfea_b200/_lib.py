@@ -64,6 +64,21 @@ class StepInfo(C.Structure):
 _vp, _dp, _i32p, _u8p, _i64p = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_uint8), C.POINTER(C.c_int64)
 _st = C.c_int
 _fp = C.POINTER(C.c_float)
+class DieGrid(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("x0", C.c_double), ("y0", C.c_double), ("dx", C.c_double),
+                ("h", C.POINTER(C.c_double))]
+
+
+class RemeshArgs(C.Structure):
+    _fields_ = [("nn", C.c_int32), ("ne", C.c_int32), ("x", C.POINTER(C.c_double)), ("tets", C.POINTER(C.c_int32)),
+                ("vg", C.POINTER(C.c_double)), ("eps", C.POINTER(C.c_double)), ("dmg", C.POINTER(C.c_double)),
+                ("sig", C.POINTER(C.c_double)), ("rate", C.POINTER(C.c_double)), ("mean", C.POINTER(C.c_double)),
+                ("bottom", DieGrid), ("top", DieGrid), ("gap", C.c_double), ("h", C.c_double), ("vol_target", C.c_double),
+                ("sym_x", C.c_int32), ("sym_y", C.c_int32), ("recovery_pass", C.c_int32),
+                ("refinement_levels", C.c_int32), ("max_nodes", C.c_int32), ("sig_ref", C.c_double),
+                ("n_hot", C.c_int32), ("hot", C.POINTER(C.c_double))]
+
+
 INSIDE_FN = C.CFUNCTYPE(C.c_int32, C.c_double, C.c_double, C.c_double, C.c_void_p)
 SIZE_FN = C.CFUNCTYPE(C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p)
 
@@ -134,6 +149,12 @@ SIGNATURES = {
     "ifea_tetmesh_tet_count": (C.c_int32, [_vp]),
     "ifea_tetmesh_get": (_st, [_vp, _dp, _i32p]),
     "ifea_tetmesh_destroy": (None, [_vp]),
+    "ifea_remesh_workpiece": (_st, [C.POINTER(RemeshArgs), C.POINTER(_vp)]),
+    "ifea_remesh_node_count": (C.c_int32, [_vp]),
+    "ifea_remesh_tet_count": (C.c_int32, [_vp]),
+    "ifea_remesh_why": (C.c_char_p, [_vp]),
+    "ifea_remesh_get": (_st, [_vp, _dp, _i32p, _u8p, _u8p, _u8p, _dp, _dp, _dp, _dp, _dp, _dp]),
+    "ifea_remesh_destroy": (None, [_vp]),
 }
 
 _LIB = None

@@ -1064,3 +1064,62 @@ ifea_status ifea_tetmesh_get(const ifea_tetmesh *m, double *x, int32_t *tets)
 void ifea_tetmesh_destroy(ifea_tetmesh *m) { delete m; }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ C ABI (RemeshCore on host arrays)
+
+struct ifea_remesh_result {
+    ifea::RemeshOutput out;
+};
+
+extern "C" {
+
+ifea_status ifea_remesh_workpiece(const ifea_remesh_args *a, ifea_remesh_result **out)
+{
+    if (!a || !out || a->nn <= 0 || a->ne <= 0 || !a->x || !a->tets || !a->vg || !a->eps || !a->dmg || !a->sig ||
+        !a->rate || !a->mean || !a->bottom.h || !a->top.h || (a->n_hot > 0 && !a->hot))
+        return IFEA_INPUT_INVALID;
+    *out = nullptr;
+    try {
+        ifea::RemeshInput in;
+        in.nn = a->nn; in.ne = a->ne; in.x = a->x; in.tets = a->tets; in.vg = a->vg;
+        in.eps = a->eps; in.dmg = a->dmg; in.sig = a->sig; in.rate = a->rate; in.mean = a->mean;
+        const ifea_die_grid *g[2] = {&a->bottom, &a->top};
+        for (int k = 0; k < 2; k++) {
+            in.die[k].side = k; in.die[k].nx = g[k]->nx; in.die[k].ny = g[k]->ny;
+            in.die[k].x0 = g[k]->x0; in.die[k].y0 = g[k]->y0; in.die[k].dx = g[k]->dx; in.die[k].h = g[k]->h;
+        }
+        in.gap = a->gap; in.h = a->h; in.vol_target = a->vol_target; in.sym_x = a->sym_x != 0; in.sym_y = a->sym_y != 0;
+        in.recovery_pass = a->recovery_pass; in.refinement_levels = a->refinement_levels; in.max_nodes = a->max_nodes;
+        in.sig_ref = a->sig_ref;
+        for (int k = 0; k < a->n_hot; k++)
+            in.hot.push_back({mk3(a->hot[4 * k], a->hot[4 * k + 1], a->hot[4 * k + 2]), (int)a->hot[4 * k + 3]});
+        auto *r = new ifea_remesh_result;
+        bool ok = ifea::remesh_workpiece(in, r->out);
+        *out = r;
+        return ok ? IFEA_OK : IFEA_MESH_DISTORTED;
+    } catch (...) {
+        return IFEA_CUDA_ERROR;
+    }
+}
+
+int32_t ifea_remesh_node_count(const ifea_remesh_result *r) { return r ? (int32_t)(r->out.x.size() / 3) : 0; }
+int32_t ifea_remesh_tet_count(const ifea_remesh_result *r) { return r ? (int32_t)(r->out.tets.size() / 4) : 0; }
+const char *ifea_remesh_why(const ifea_remesh_result *r) { return r ? r->out.why.c_str() : ""; }
+
+ifea_status ifea_remesh_get(const ifea_remesh_result *r, double *x, int32_t *tets, uint8_t *on_x0, uint8_t *on_y0,
+                            uint8_t *contact, double *vg, double *eps, double *dmg, double *sig, double *rate,
+                            double *mean)
+{
+    if (!r || r->out.tets.empty()) return IFEA_BAD_STATE;
+    const ifea::RemeshOutput &o = r->out;
+    auto cp = [](auto *dst, const auto &v) {
+        if (dst) std::copy(v.begin(), v.end(), dst);
+    };
+    cp(x, o.x); cp(tets, o.tets); cp(on_x0, o.on_x0); cp(on_y0, o.on_y0); cp(contact, o.contact); cp(vg, o.vg);
+    cp(eps, o.eps); cp(dmg, o.dmg); cp(sig, o.sig); cp(rate, o.rate); cp(mean, o.mean);
+    return IFEA_OK;
+}
+
+void ifea_remesh_destroy(ifea_remesh_result *r) { delete r; }
+
+}  // extern "C"

@@ -173,6 +173,37 @@ ifea_status ifea_tetmesh_get(const ifea_tetmesh *m, double *x, int32_t *tets);
 void ifea_tetmesh_destroy(ifea_tetmesh *m);
 /* why the last remesh of the context was rejected, or what the last accepted one made */
 const char *ifea3d_last_remesh(const ifea3d *ctx);
+/* RemeshCore itself on host arrays, for a host that steps the increments elsewhere (the C# solver's Remesh, or a
+ * CPU solver): the deformed mesh and its state in, the new mesh and the remapped state out. Returns IFEA_OK when
+ * the new mesh is accepted, IFEA_MESH_DISTORTED when rejected (ifea_remesh_why says why). */
+typedef struct ifea_die_grid {
+    int32_t nx, ny;
+    double x0, y0, dx;
+    const double *h;              /* (nx + 1) * (ny + 1) heights, row-major in y; the top die at its closed place */
+} ifea_die_grid;
+typedef struct ifea_remesh_args {
+    int32_t nn, ne;
+    const double *x;              /* 3 per node */
+    const int32_t *tets;          /* 4 per tet */
+    const double *vg;             /* global velocity, 3 per node */
+    const double *eps, *dmg, *sig, *rate, *mean;   /* per tet */
+    ifea_die_grid bottom, top;
+    double gap, h, vol_target;    /* die gap, element size, initial volume of the modelled part */
+    int32_t sym_x, sym_y, recovery_pass, refinement_levels, max_nodes;
+    double sig_ref;               /* flow stress where no old element is found */
+    int32_t n_hot;
+    const double *hot;            /* 4 per failure place: x, y, z, refinement level */
+} ifea_remesh_args;
+typedef struct ifea_remesh_result ifea_remesh_result;
+ifea_status ifea_remesh_workpiece(const ifea_remesh_args *args, ifea_remesh_result **out);
+int32_t ifea_remesh_node_count(const ifea_remesh_result *r);
+int32_t ifea_remesh_tet_count(const ifea_remesh_result *r);
+const char *ifea_remesh_why(const ifea_remesh_result *r);
+/* any output pointer may be NULL */
+ifea_status ifea_remesh_get(const ifea_remesh_result *r, double *x, int32_t *tets, uint8_t *on_x0, uint8_t *on_y0,
+                            uint8_t *contact, double *vg, double *eps, double *dmg, double *sig, double *rate,
+                            double *mean);
+void ifea_remesh_destroy(ifea_remesh_result *r);
 
 /* ------------------------------------------------------------------ learned warm start (3D)
  *

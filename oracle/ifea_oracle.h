@@ -57,6 +57,13 @@ int o3d_set_die(o3d *s, int side, int nx, int ny, double x0, double y0, double d
 int o3d_init(o3d *s, double gap0, double min_x, double min_y, double min_z, double max_x, double max_y);
 /* One increment (Forging3DSolver.Step). */
 int o3d_step(o3d *s);
+/* remeshing through the host's remesher: fn(user, s) reads the state (o3d_array / o3d_scalar), installs the new
+ * mesh with o3d_replace_mesh and returns 1, or returns 0 when it rejects the new mesh */
+typedef int (*o3d_remesh_fn)(void *user, o3d *s);
+void o3d_set_remesher(o3d *s, o3d_remesh_fn fn, void *user);
+int o3d_replace_mesh(o3d *s, int nn, int ne, const double *x, const int32_t *tets, const uint8_t *on_x0,
+                     const uint8_t *on_y0, const uint8_t *contact, const double *vg, const double *eps,
+                     const double *dmg, const double *sig, const double *rate, const double *mean);
 
 /* Lower-level entry points for teacher-forced parity. */
 int o3d_prepare_step(o3d *s);

@@ -55,6 +55,12 @@ struct o3d {
     int lin_its_total;
     double load, reaction, power, rnorm_last, beta_last, max_diag_last;
     char err[512];
+    /* remeshing: the host's remesher, called where Step remeshes (ThreeD/Forging3DSolver.cs:544-611) */
+    o3d_remesh_fn remesh_cb;
+    void *remesh_user;
+    int remesh_count, refinement_levels, max_nodes, nhot, have_fail_at;
+    double fail_at[3];
+    double hot[4 * 64];            /* places where increments failed: x, y, z, refinement level */
 };
 
 static int fail(o3d *s, int code, const char *msg)
@@ -77,6 +83,8 @@ o3d *o3d_create(const o3d_params *p)
     s->sig_ref = law_stress(p->C, p->N, p->M, p->eps0, 0, s->rate_ref);
     s->k_pen = p->penalty_factor * s->sig_ref / s->rate_ref;
     s->u0 = 5e-3 * p->ram;
+    s->refinement_levels = 1;
+    s->max_nodes = 1 << 30;
     s->lin = ospd_create();
     s->need_analyze = 1;
     return s;
@@ -84,13 +92,25 @@ o3d *o3d_create(const o3d_params *p)
 
 static void free_mesh(o3d *s)
 {
-    void *ptrs[] = {s->tets, s->on_x0, s->on_y0, s->is_surface, s->nts, s->ntl, s->bface, s->bowner, s->bsym,
-                    s->nbr_start, s->nbr, s->col_ptr, s->row_idx, s->e_nbr, s->h_local, s->x, s->vg, s->vg_prev,
-                    s->eps, s->dmg, s->el_dev, s->el_sig, s->el_rate, s->el_mean, s->contact, s->release, s->fixed,
-                    s->ax, s->n_fix, s->die_axis, s->fixed_val, s->k_fric, s->a_fric, s->grad, s->vol, s->v, s->r,
-                    s->dv, s->v_trial, s->rvol, s->v_node, s->g_start, s->g_node, s->g_coef, s->kvol, s->val, s->e_r,
-                    s->e_k, s->e_energy, s->e_power, s->pr, s->pz, s->pp, s->pq};
-    for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); k++) free(ptrs[k]);
+    /* every pointer is cleared too: a mesh replaced by a remesh must not leave one behind to be freed twice */
+    void **ptrs[] = {(void **)&s->tets, (void **)&s->on_x0, (void **)&s->on_y0, (void **)&s->is_surface,
+                     (void **)&s->nts, (void **)&s->ntl, (void **)&s->bface, (void **)&s->bowner, (void **)&s->bsym,
+                     (void **)&s->nbr_start, (void **)&s->nbr, (void **)&s->col_ptr, (void **)&s->row_idx,
+                     (void **)&s->e_nbr, (void **)&s->h_local, (void **)&s->x, (void **)&s->vg, (void **)&s->vg_prev,
+                     (void **)&s->eps, (void **)&s->dmg, (void **)&s->el_dev, (void **)&s->el_sig,
+                     (void **)&s->el_rate, (void **)&s->el_mean, (void **)&s->contact, (void **)&s->release,
+                     (void **)&s->fixed, (void **)&s->ax, (void **)&s->n_fix, (void **)&s->die_axis,
+                     (void **)&s->fixed_val, (void **)&s->k_fric, (void **)&s->a_fric, (void **)&s->grad,
+                     (void **)&s->vol, (void **)&s->v, (void **)&s->r, (void **)&s->dv, (void **)&s->v_trial,
+                     (void **)&s->rvol, (void **)&s->v_node, (void **)&s->g_start, (void **)&s->g_node,
+                     (void **)&s->g_coef, (void **)&s->kvol, (void **)&s->val, (void **)&s->e_r, (void **)&s->e_k,
+                     (void **)&s->e_energy, (void **)&s->e_power, (void **)&s->pr, (void **)&s->pz, (void **)&s->pp,
+                     (void **)&s->pq};
+    for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); k++) {
+        free(*ptrs[k]);
+        *ptrs[k] = NULL;
+    }
+    s->g_len = 0;
 }
 
 void o3d_destroy(o3d *s)
@@ -1156,6 +1176,11 @@ int o3d_try_update(o3d *s, double dt, int *ok)
     smooth_interior(s, xT, 0.05, 6);
     for (int e = 0; e < s->ne; e++) {
         if (tet_quality_x(s, xT, e) <= 0.005) {
+            /* the failure point for local refinement at the next remesh (_failAt, :1517) */
+            for (int c = 0; c < 3; c++)
+                s->fail_at[c] = 0.25 * (xT[3 * s->tets[4 * e] + c] + xT[3 * s->tets[4 * e + 1] + c] +
+                                        xT[3 * s->tets[4 * e + 2] + c] + xT[3 * s->tets[4 * e + 3] + c]);
+            s->have_fail_at = 1;
             char msg[120];
             snprintf(msg, sizeof msg, "tetrahedron %d collapsed", e);
             free(xT); free(pred); free(nrm); free(cT);
@@ -1178,18 +1203,57 @@ static double min_quality(const o3d *s)
     return q;
 }
 
-/* RemeshTrigger (:1867-1883): first-aid smoothing, then count what would have remeshed */
-static void remesh_trigger(o3d *s)
+/* RemeshTrigger (:1867-1883): first-aid smoothing, then whether a remesh is due (counted as a request) */
+static int remesh_trigger(o3d *s)
 {
     if (min_quality(s) < s->p.remesh_quality) smooth_interior(s, s->x, s->p.remesh_quality, 6);
-    if (min_quality(s) < s->p.remesh_quality) { s->remesh_requests++; return; }
+    if (min_quality(s) < s->p.remesh_quality) { s->remesh_requests++; return 1; }
     double maxEdge = 0;
     for (int k = 0; k < 3 * s->nbf; k += 3) {
         const int32_t *f = s->bface;
         maxEdge = dmax(maxEdge, dmax(vlen(vsub(X(s, f[k + 1]), X(s, f[k]))),
                                      dmax(vlen(vsub(X(s, f[k + 2]), X(s, f[k + 1]))), vlen(vsub(X(s, f[k]), X(s, f[k + 2]))))));
     }
-    if (maxEdge > 2.8 * s->h) s->remesh_requests++;
+    if (maxEdge > 2.8 * s->h) { s->remesh_requests++; return 1; }
+    return 0;
+}
+
+/* Remesh (:1945-1956): the host's remesher replaces the mesh and state (o3d_replace_mesh) and returns 1, or
+ * rejects the new mesh and returns 0; without a remesher the request stays only counted */
+static int remesh(o3d *s)
+{
+    if (!s->remesh_cb) return 0;
+    int ok = s->remesh_cb(s->remesh_user, s);
+    if (ok) s->remesh_count++;
+    return ok;
+}
+
+void o3d_set_remesher(o3d *s, o3d_remesh_fn fn, void *user)
+{
+    s->remesh_cb = fn;
+    s->remesh_user = user;
+}
+
+/* the new mesh and the state remapped onto it (RemeshCore's Allocate and field hand-over, :2042-2057); the
+ * increment state (gap, time, step, counters) stays, the next increment starts cold (_warm = false) */
+int o3d_replace_mesh(o3d *s, int nn, int ne, const double *x, const int32_t *tets, const uint8_t *on_x0,
+                     const uint8_t *on_y0, const uint8_t *contact, const double *vg, const double *eps,
+                     const double *dmg, const double *sig, const double *rate, const double *mean)
+{
+    int rc = o3d_set_mesh(s, nn, ne, x, tets, on_x0, on_y0);
+    if (rc != E_OK) return rc;
+    memcpy(s->contact, contact, nn);
+    memcpy(s->vg, vg, sizeof(double) * 3 * nn);
+    memcpy(s->eps, eps, sizeof(double) * ne);
+    memcpy(s->dmg, dmg, sizeof(double) * ne);
+    memcpy(s->el_sig, sig, sizeof(double) * ne);
+    memcpy(s->el_rate, rate, sizeof(double) * ne);
+    memcpy(s->el_mean, mean, sizeof(double) * ne);
+    s->have_vg_prev = 0;
+    s->warm = 0;
+    s->pcg_failures = 0;
+    s->pcg_skip = 0;
+    return E_OK;
 }
 
 /* LayerLimitedIncrement (:236-249) */
@@ -1223,7 +1287,7 @@ int o3d_step(o3d *s)
 {
     if (s->gap <= 1e-9) return fail(s, E_STATE, "Simulation already reached the closed-die position.");
     s->step_index++;
-    remesh_trigger(s);
+    if (remesh_trigger(s)) remesh(s);
     double step_cap = s->p.ds * s->h / s->p.h;
     int iterations = 0, ok = 0, used_cutback = 0, rc;
     double load = 0, reaction = 0, dt = 0;
@@ -1238,7 +1302,10 @@ int o3d_step(o3d *s)
             if (s->last_rel < 1e-2) {
                 /* warning: not fully converged; continuing */
             } else {
-                if (pass < passes - 1) s->remesh_requests++; /* Remesh("stalled velocity solution") unavailable */
+                if (pass < passes - 1) {
+                    s->remesh_requests++;
+                    if (remesh(s)) continue; /* Remesh("stalled velocity solution") */
+                }
                 char msg[200];
                 snprintf(msg, sizeof msg, "Velocity solution did not converge at step %d (stroke %.3f mm): |dv|/|v| = %.2e.",
                          s->step_index, s->gap0 - s->gap, s->last_rel);
@@ -1258,7 +1325,17 @@ int o3d_step(o3d *s)
             if (ok) { dt = dta; used_cutback = attempt; }
         }
         if (ok || pass == passes - 1) break;
-        s->remesh_requests++; /* Remesh(...) would run here; unavailable, so the ladder continues */
+        if (pass >= 1 && s->refinement_levels > 0 && s->have_fail_at) {
+            if (s->nhot == 64) {
+                memmove(s->hot, s->hot + 4, sizeof(double) * 4 * 63);
+                s->nhot--;
+            }
+            double *hs = s->hot + 4 * s->nhot++;
+            hs[0] = s->fail_at[0]; hs[1] = s->fail_at[1]; hs[2] = s->fail_at[2];
+            hs[3] = imin(pass, s->refinement_levels);
+        }
+        s->remesh_requests++;
+        remesh(s); /* a rejected remesh does not end the ladder */
     }
     s->recovery_pass = 0;
     if (!ok) {
@@ -1286,6 +1363,7 @@ void *o3d_array(o3d *s, const char *name, int64_t *count)
 {
 #define ARR(nm, ptr, cnt) if (!strcmp(name, nm)) { *count = (cnt); return (void *)(ptr); }
     ARR("x", s->x, 3 * (int64_t)s->nn)
+    ARR("hot", s->hot, 4 * (int64_t)s->nhot)
     ARR("vg", s->vg, 3 * (int64_t)s->nn)
     ARR("eps", s->eps, s->ne)
     ARR("dmg", s->dmg, s->ne)
@@ -1346,6 +1424,8 @@ double o3d_scalar(o3d *s, const char *name)
     SC("pcg_skip", s->pcg_skip) SC("pcg_failures", s->pcg_failures) SC("lin_its", s->lin_its_total)
     SC("nbf", s->nbf) SC("min_quality", min_quality(s)) SC("recovery_pass", s->recovery_pass)
     SC("factor_nnz", ospd_factor_nonzeros(s->lin))
+    SC("remesh_count", s->remesh_count) SC("refinement_levels", s->refinement_levels) SC("max_nodes", s->max_nodes)
+    SC("h", s->h) SC("nn", s->nn) SC("ne", s->ne)
 #undef SC
     return NAN;
 }
@@ -1356,5 +1436,7 @@ int o3d_set_scalar(o3d *s, const char *name, double v)
     if (!strcmp(name, "recovery_pass")) { s->recovery_pass = (int)v; return 0; }
     if (!strcmp(name, "ds_cur")) { s->ds_cur = v; return 0; }
     if (!strcmp(name, "warm")) { s->warm = (int)v; return 0; }
+    if (!strcmp(name, "refinement_levels")) { s->refinement_levels = (int)v; return 0; }
+    if (!strcmp(name, "max_nodes")) { s->max_nodes = (int)v; return 0; }
     return -1;
 }

@@ -43,6 +43,9 @@ class O2DParams(C.Structure):
                 ("height", C.c_double), ("nx", C.c_int), ("nz", C.c_int)]
 
 
+REMESH_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p)
+
+
 def _declare(L):
     vp, dp, ip, i32p, u8p = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int32), C.POINTER(C.c_uint8)
     i64p = C.POINTER(C.c_int64)
@@ -60,12 +63,15 @@ def _declare(L):
         "o3d_die_project": (C.c_double, [vp, C.c_int, dp, C.c_double, dp, dp]),
         "o3d_die_clearance": (C.c_double, [vp, C.c_int, dp, C.c_double]),
         "o3d_tet_quality": (C.c_double, [dp, dp, dp, dp]),
+        "o3d_set_remesher": (None, [vp, REMESH_FN, vp]),
+        "o3d_replace_mesh": (C.c_int, [vp, C.c_int, C.c_int, dp, i32p, u8p, u8p, u8p, dp, dp, dp, dp, dp, dp]),
         "o_flow_stress": (C.c_double, [C.c_double] * 6),
         "o_principal_max3": (C.c_double, [C.c_double] * 6),
         "ospd_create": (vp, []), "ospd_destroy": (None, [vp]),
         "ospd_analyze": (C.c_int, [vp, C.c_int, i32p, i32p]), "ospd_factorize": (C.c_int, [vp, dp]),
         "ospd_solve": (C.c_int, [vp, dp, dp]), "ospd_factor_nonzeros": (C.c_int64, [vp]),
         "ospd_bad_pivot": (C.c_int, [vp]),
+        "ospd_set_geometry": (None, [vp, C.c_int, dp]),
         "oband_create": (vp, [C.c_int, C.c_int]), "oband_destroy": (None, [vp]), "oband_bandwidth": (C.c_int, [vp]),
         "oband_add": (C.c_int, [vp, C.c_int, C.c_int, C.c_double]), "oband_get": (C.c_double, [vp, C.c_int, C.c_int]),
         "oband_constrain": (None, [vp, C.c_int]), "oband_clear": (None, [vp]),
@@ -114,6 +120,7 @@ class Oracle3D:
                       int(cfg.sym_y), cfg.sym_factor, cfg.penalty_factor, cfg.newton_blend, int(cfg.quadratic_ls),
                       int(cfg.extrapolate_start), int(cfg.adaptive_newton), int(cfg.sticky_secant), cfg.pcg_budget)
         self.L = L
+        self.p = cfg
         self.h = L.o3d_create(C.byref(p))
         x = np.ascontiguousarray(mesh.x, np.float64)
         t = np.ascontiguousarray(mesh.tets, np.int32)
@@ -190,6 +197,51 @@ class Oracle3D:
     def set_scalar(self, name, v):
         return self.L.o3d_set_scalar(self.h, name.encode(), float(v))
 
+    def enable_remesh(self, dies):
+        """Remesh where the reference's Step remeshes, with the library's host remesher (the same host code the GPU
+        stepper calls: RemeshCore, ThreeD/Forging3DSolver.cs:1958-2101): the oracle restates the per-iteration path
+        only, and the remesh sits outside it on the host in both."""
+        from impressionfea_b200 import _lib
+
+        G = _lib.lib()
+        vol_target = self.scalar("vol0") / self.p.sym_factor
+        self._die_keep = [np.ascontiguousarray(d.h, np.float64) for d in dies]
+        grids = [_lib.DieGrid(d.nx, d.ny, d.x0, d.y0, d.dx, hh.ctypes.data_as(C.POINTER(C.c_double)))
+                 for d, hh in zip(dies, self._die_keep)]
+
+        def cb(_user, _s):
+            f64 = lambda nm: np.ascontiguousarray(self.array(nm), np.float64)
+            x, vg, eps, dmg, sig, rate, mean = (f64(n) for n in ("x", "vg", "eps", "dmg", "el_sig", "el_rate", "el_mean"))
+            tets = np.ascontiguousarray(self.array("tets"), np.int32)
+            hot = np.ascontiguousarray(self.array("hot"), np.float64)
+            dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+            args = _lib.RemeshArgs(int(len(x) // 3), int(len(tets) // 4), dp(x), tets.ctypes.data_as(C.POINTER(C.c_int32)),
+                                   dp(vg), dp(eps), dp(dmg), dp(sig), dp(rate), dp(mean), grids[0], grids[1],
+                                   self.scalar("gap"), self.scalar("h"), vol_target, int(self.p.sym_x), int(self.p.sym_y),
+                                   int(self.scalar("recovery_pass")), int(self.scalar("refinement_levels")),
+                                   int(self.scalar("max_nodes")), self.scalar("sig_ref"), len(hot) // 4, dp(hot))
+            r = C.c_void_p()
+            st = G.ifea_remesh_workpiece(C.byref(args), C.byref(r))
+            try:
+                if st != 0:
+                    return 0
+                nn, ne = G.ifea_remesh_node_count(r), G.ifea_remesh_tet_count(r)
+                out = {k: np.zeros(n, t) for k, n, t in (("x", 3 * nn, np.float64), ("tets", 4 * ne, np.int32),
+                                                         ("onx", nn, np.uint8), ("ony", nn, np.uint8), ("contact", nn, np.uint8),
+                                                         ("vg", 3 * nn, np.float64), ("eps", ne, np.float64), ("dmg", ne, np.float64),
+                                                         ("sig", ne, np.float64), ("rate", ne, np.float64), ("mean", ne, np.float64))}
+                ptr = lambda a: a.ctypes.data_as(C.POINTER(np.ctypeslib.as_ctypes_type(a.dtype)))
+                G.ifea_remesh_get(r, *(ptr(out[k]) for k in ("x", "tets", "onx", "ony", "contact", "vg", "eps", "dmg", "sig", "rate", "mean")))
+                rc = self.L.o3d_replace_mesh(self.h, nn, ne, ptr(out["x"]), ptr(out["tets"]), ptr(out["onx"]), ptr(out["ony"]),
+                                             ptr(out["contact"]), ptr(out["vg"]), ptr(out["eps"]), ptr(out["dmg"]),
+                                             ptr(out["sig"]), ptr(out["rate"]), ptr(out["mean"]))
+                return 1 if rc == 0 else 0
+            finally:
+                G.ifea_remesh_destroy(r)
+
+        self._remesh_cb = REMESH_FN(cb)
+        self.L.o3d_set_remesher(self.h, self._remesh_cb, None)
+
     def die_project(self, side, p, offset):
         p = np.ascontiguousarray(p, np.float64)
         q = np.zeros(3)
@@ -208,6 +260,11 @@ class OracleSpd:
     def __init__(self):
         self.L = lib()
         self.h = self.L.ospd_create()
+
+    def set_geometry(self, xyz):
+        """Node coordinates (3 per node) for the coordinate nested-dissection order of the next analysis."""
+        self._xyz = np.ascontiguousarray(xyz, np.float64)
+        self.L.ospd_set_geometry(self.h, len(self._xyz) // 3, _dp(self._xyz))
 
     def analyze(self, n, col_ptr, row_idx):
         self._cp = np.ascontiguousarray(col_ptr, np.int32)

@@ -233,3 +233,24 @@ def test_2d_upsetting_80_increments_track_the_oracle():
                 assert "distortion" in str(err).lower()
                 stop_ora = k
     assert stop_gpu == stop_ora
+
+
+# ------------------------------------------------------------------ remeshing on both sides
+
+def test_remeshing_runs_track_the_oracle():
+    # a small gear blank with the remesh threshold raised so that every increment remeshes: the GPU stepper and the
+    # oracle both call the library's host remesher (RemeshCore) at the same points of Step; the state they hand it
+    # differs only by rounding, so the new meshes and the loads on them agree
+    cfg, mesh, dies = closed_die_gear_blank(target_tets=5000)
+    cfg = dataclasses.replace(cfg, remesh_quality=0.4)
+    gpu, ora = Forging3DSolver(cfg, mesh, dies), Oracle3D(cfg, mesh, dies)
+    gpu.set_scalar("remesh", 1)
+    ora.enable_remesh(dies)
+    for k in range(1, 4):
+        info = gpu.step()
+        ora.step()
+        assert gpu.scalar("remesh_count") == ora.scalar("remesh_count") == k, f"increment {k}: remeshes"
+        assert gpu.scalar("ne") == ora.scalar("ne"), f"increment {k}: tets after the remesh"
+        assert abs(info["load"] / ora.scalar("load") - 1) < 1e-4, f"increment {k}: load"
+        np.testing.assert_array_equal(gpu.array("contact"), ora.array("contact"), err_msg=f"increment {k}: contact")
+    gpu.close()
