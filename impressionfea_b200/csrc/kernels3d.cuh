@@ -19,7 +19,7 @@ enum AsmMode { ASM_MATRIX = 0, ASM_RESIDUAL = 1, ASM_ENERGY = 2 };
 enum Slot {
     S_E_VOL = 0, S_E_ELEM, S_E_FRIC, S_P_ELEM, S_P_FRIC, S_MAXDIAG, S_RNORM2, S_DOT, S_NORM_A, S_NORM_B,
     S_REACTION, S_MAX_B, S_MAX_T, S_KEPT_B, S_KEPT_T, S_MAXPEN, S_MINQ, S_VOLUME, S_MAXEDGE, S_THIN,
-    S_RZ, S_RZNEW, S_PQ, S_RR, S_BB,
+    S_RZ, S_RZNEW, S_PQ, S_RR, S_BB, S_FILL, S_BOX0, S_BOX1, S_BOX2, S_BOX3, S_BOX4, S_BOX5,
     S_COUNT
 };
 

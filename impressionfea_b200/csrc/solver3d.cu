@@ -106,10 +106,136 @@ __global__ void k_ws_guess(View3 V, const double *__restrict__ v0, const float *
     }
 }
 
+// One pass of low-pass filtering of the predicted velocity change over the mesh: each node takes the mean, over its
+// tets, of the tets' nodal means. The network predicts every node on its own; its pointwise noise is not
+// divergence-free and the penalty term of the functional punishes exactly that, so the prediction is smoothed
+// before it is weighed against the reference start.
+__global__ void k_ws_smooth(View3 V, const float *__restrict__ Y, float *__restrict__ out)
+{
+    GRID_STRIDE(n, V.nn)
+    {
+        float acc[3] = {0, 0, 0};
+        int cnt = V.nts[n + 1] - V.nts[n];
+        for (int32_t q = V.nts[n]; q < V.nts[n + 1]; q++) {
+            const int32_t *t = V.tets + 4 * (int64_t)V.ntl[q];
+            for (int a = 0; a < 4; a++)
+                for (int c = 0; c < 3; c++) acc[c] += 0.25f * Y[3 * (int64_t)t[a] + c];
+        }
+        for (int c = 0; c < 3; c++) out[3 * (int64_t)n + c] = cnt ? acc[c] / cnt : Y[3 * (int64_t)n + c];
+    }
+}
+
 // out = a + s (b - a), elementwise
 __global__ void k_ws_mix(int n, const double *__restrict__ a, const double *__restrict__ b, double s, double *__restrict__ out)
 {
     GRID_STRIDE(i, n) { out[i] = a[i] + s * (b[i] - a[i]); }
+}
+
+// ------------------------------------------------------------------ FillPercent (:2149-2189) on the device
+// The reference builds a TetLocator over the current mesh every step (a bucket grid of cell 2 h over the nodes'
+// bounding box, every tet listed in each cell its bounding box touches) and counts the closed cavity's sample points
+// that lie in some tet (barycentric weights all >= -1e-9 in a tet of positive volume). Here the grid is built by
+// counting, a one-block prefix sum and a fill, and one thread tests each sample point against its cell's tets.
+struct LocGrid {
+    double x0, y0, z0, cell;
+    int nx, ny, nz;
+};
+
+__global__ void k_node_box(View3 V)
+{
+    double mx[6] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    GRID_STRIDE(n, V.nn)
+    {
+        d3 p = ld3(V.x, n);
+        mx[0] = rmax(mx[0], p.x); mx[1] = rmax(mx[1], p.y); mx[2] = rmax(mx[2], p.z);
+        mx[3] = rmax(mx[3], -p.x); mx[4] = rmax(mx[4], -p.y); mx[5] = rmax(mx[5], -p.z);
+    }
+    const int s6[6] = {S_BOX0, S_BOX1, S_BOX2, S_BOX3, S_BOX4, S_BOX5};
+    emit_max<6>(V, mx, s6);
+}
+
+__device__ __forceinline__ int loc_axis(double v, double v0, double cell, int n)
+{
+    return iclamp((int)((v - v0) / cell), 0, n - 1);
+}
+
+// mode 0: count the tets of every cell (into count[c + 1]); mode 1: list them (slot from fill[c])
+__global__ void k_loc_tets(View3 V, LocGrid G, int mode, int32_t *__restrict__ count, int32_t *__restrict__ fill,
+                           int32_t *__restrict__ items)
+{
+    GRID_STRIDE(e, V.ne)
+    {
+        const int32_t *t = V.tets + 4 * e;
+        d3 lo = ld3(V.x, t[0]), hi = lo;
+        for (int a = 1; a < 4; a++) {
+            d3 p = ld3(V.x, t[a]);
+            lo = mk3(rmin(lo.x, p.x), rmin(lo.y, p.y), rmin(lo.z, p.z));
+            hi = mk3(rmax(hi.x, p.x), rmax(hi.y, p.y), rmax(hi.z, p.z));
+        }
+        int i0 = loc_axis(lo.x, G.x0, G.cell, G.nx), i1 = loc_axis(hi.x, G.x0, G.cell, G.nx);
+        int j0 = loc_axis(lo.y, G.y0, G.cell, G.ny), j1 = loc_axis(hi.y, G.y0, G.cell, G.ny);
+        int k0 = loc_axis(lo.z, G.z0, G.cell, G.nz), k1 = loc_axis(hi.z, G.z0, G.cell, G.nz);
+        for (int k = k0; k <= k1; k++)
+            for (int j = j0; j <= j1; j++)
+                for (int i = i0; i <= i1; i++) {
+                    int c = (k * G.ny + j) * G.nx + i;
+                    if (mode == 0) atomicAdd(count + c + 1, 1);
+                    else items[atomicAdd(fill + c, 1)] = e;
+                }
+    }
+}
+
+// inclusive prefix sum of a[0..n) in one block (n is a few thousand cells), fill = a copy of it
+__global__ void k_scan_block(int32_t *__restrict__ a, int n, int32_t *__restrict__ fill)
+{
+    __shared__ int32_t carry;
+    __shared__ int32_t part[1024];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += 1024) {
+        int i = base + threadIdx.x;
+        part[threadIdx.x] = i < n ? a[i] : 0;
+        __syncthreads();
+        for (int off = 1; off < 1024; off <<= 1) {
+            int32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
+            __syncthreads();
+            part[threadIdx.x] += v;
+            __syncthreads();
+        }
+        if (i < n) {
+            a[i] = part[threadIdx.x] + carry;
+            fill[i] = a[i];
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += part[1023];
+        __syncthreads();
+    }
+}
+
+__global__ void k_fill_query(View3 V, LocGrid G, const int32_t *__restrict__ start, const int32_t *__restrict__ items,
+                             const double *__restrict__ pts, int np)
+{
+    double acc[1] = {0};
+    GRID_STRIDE(q, np)
+    {
+        d3 p = ld3(pts, q);
+        int c = (loc_axis(p.z, G.z0, G.cell, G.nz) * G.ny + loc_axis(p.y, G.y0, G.cell, G.ny)) * G.nx +
+                loc_axis(p.x, G.x0, G.cell, G.nx);
+        for (int32_t k = start[c]; k < start[c + 1]; k++) {
+            const int32_t *t = V.tets + 4 * items[k];
+            d3 a = ld3(V.x, t[0]), b = ld3(V.x, t[1]), cc = ld3(V.x, t[2]), d = ld3(V.x, t[3]);
+            double v = tet_volume(a, b, cc, d);
+            if (v <= 0) continue;
+            double b0 = tet_volume(p, b, cc, d) / v, b1 = tet_volume(a, p, cc, d) / v, b2 = tet_volume(a, b, p, d) / v;
+            double b3 = 1 - b0 - b1 - b2;
+            if (b0 >= -1e-9 && b1 >= -1e-9 && b2 >= -1e-9 && b3 >= -1e-9) {
+                acc[0] += 1;
+                break;
+            }
+        }
+    }
+    const int s1[1] = {S_FILL};
+    emit_sum<1>(V, acc, s1);
 }
 
 struct PhaseTimer {
@@ -170,13 +296,16 @@ struct Forging3D {
     bool have_fail_at = false;
     std::vector<double> die_host[2];  // host copies of the die heights (the remesher's clearances)
     std::string last_remesh;
+    DBuf<double> d_cavity;          // the closed cavity's sample points (FillPercent)
+    DBuf<int32_t> d_loc_start, d_loc_fill, d_loc_items;
     WarmStartNet *ws_net = nullptr;
     int ws_mode = 0, ws_used = 0, ws_fallbacks = 0;
     // 0: the lower-functional start of the two; 1: the network's start always; 2: a step along the prediction
     // from the reference start, chosen on the functional (the reference start when no step lowers it)
     int ws_policy = 0;
+    int ws_smooth = 2;  // smoothing passes over the prediction (k_ws_smooth)
     double ws_last_step = 0;
-    DBuf<float> d_wsf, d_wst, d_wsy;
+    DBuf<float> d_wsf, d_wst, d_wsy, d_wsy2;
     DBuf<double> d_wsv0, d_wstry;
     int pcg_failures = 0, pcg_skip = 0, pcg_failures_total = 0;
     // mesh
@@ -516,6 +645,13 @@ struct Forging3D {
         if (!(ws_mode & 2) || !warm || !have_vg_prev) return;
         d_wsy.resize((size_t)3 * nn);
         ws_net->infer_device(d_wsf, nn, d_wsy, st);
+        if (ws_smooth > 0) {
+            d_wsy2.resize((size_t)3 * nn);
+            for (int p = 0; p < ws_smooth; p++) {
+                k_ws_smooth<<<grid(nn), 256, 0, st>>>(V, d_wsy, d_wsy2);
+                std::swap(d_wsy.p, d_wsy2.p);
+            }
+        }
         k_ws_guess<<<grid(nn), 256, 0, st>>>(V, d_wsv0, d_wsy, d_vbuf[1 - vcur]);
         if (ws_policy == 1) {  // the network's start, unconditionally
             vcur = 1 - vcur;
@@ -883,6 +1019,44 @@ struct Forging3D {
         return true;
     }
 
+    // ---------------------------------------------------------------- FillPercent (:2149-2189)
+    void set_cavity(int n, const double *xyz)
+    {
+        if (n < 0 || (n > 0 && !xyz)) throw Failure(IFEA_INPUT_INVALID, "invalid cavity samples");
+        d_cavity.upload(xyz, 3 * (size_t)n, st);
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    }
+
+    double fill_percent()
+    {
+        int np = (int)(d_cavity.n / 3);
+        if (np == 0) return 0;
+        View3 V = view();
+        k_node_box<<<kReduceBlocks, 256, 0, st>>>(V);
+        finalize({MAXS(S_BOX0), MAXS(S_BOX1), MAXS(S_BOX2), MAXS(S_BOX3), MAXS(S_BOX4), MAXS(S_BOX5)});
+        const double *b = read_scalars();
+        LocGrid G;
+        G.cell = 2 * h;
+        G.x0 = -b[S_BOX3] - G.cell; G.y0 = -b[S_BOX4] - G.cell; G.z0 = -b[S_BOX5] - G.cell;
+        G.nx = (int)((b[S_BOX0] - G.x0) / G.cell) + 2;
+        G.ny = (int)((b[S_BOX1] - G.y0) / G.cell) + 2;
+        G.nz = (int)((b[S_BOX2] - G.z0) / G.cell) + 2;
+        int ncell = G.nx * G.ny * G.nz;
+        d_loc_start.resize(ncell + 1);
+        d_loc_fill.resize(ncell + 1);
+        d_loc_start.zero(st);
+        k_loc_tets<<<grid(topo.ne), 256, 0, st>>>(V, G, 0, d_loc_start, nullptr, nullptr);
+        k_scan_block<<<1, 1024, 0, st>>>(d_loc_start, ncell + 1, d_loc_fill);
+        int32_t total = 0;
+        cuda_check(cudaMemcpyAsync(&total, d_loc_start.p + ncell, sizeof total, cudaMemcpyDeviceToHost, st), "D2H");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        d_loc_items.resize(std::max(total, 1));
+        k_loc_tets<<<grid(topo.ne), 256, 0, st>>>(V, G, 1, nullptr, d_loc_fill, d_loc_items);
+        k_fill_query<<<kReduceBlocks, 256, 0, st>>>(V, G, d_loc_start, d_loc_items, d_cavity, np);
+        finalize({S_FILL});
+        return 100.0 * read_scalars()[S_FILL] / np;
+    }
+
     // ---------------------------------------------------------------- Remesh (:1945-2101)
     bool remesh(const std::string &reason)
     {
@@ -1104,12 +1278,13 @@ struct Forging3D {
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
         S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows) S("tc_updates", lin->tc_launches())
         S("factor_gflop", factor_gflop())
-        S("ws_used", ws_used) S("ws_fallbacks", ws_fallbacks) S("ws_mode", ws_mode) S("ws_policy", ws_policy)
+        S("ws_used", ws_used) S("ws_fallbacks", ws_fallbacks) S("ws_mode", ws_mode) S("ws_policy", ws_policy) S("ws_smooth", ws_smooth)
         S("ws_last_step", ws_last_step)
         S("remesh", remesh_enabled) S("remesh_count", remesh_count) S("remesh_rejected", remesh_rejected)
         S("t_remesh", t_remesh) S("refinement_levels", refinement_levels) S("max_nodes", max_nodes) S("hot_spots", hot.size())
 #undef S
         if (nm == "volume") return volume();
+        if (nm == "fill_percent") return fill_percent();
         if (nm == "min_quality") return min_quality(d_x);
         throw Failure(IFEA_INPUT_INVALID, "unknown scalar name '" + nm + "'");
     }
@@ -1132,6 +1307,7 @@ struct Forging3D {
             pcg_early_abort = v != 0;
         } else if (nm == "pcg_early_abort") pcg_early_abort = v != 0;
         else if (nm == "remesh") remesh_enabled = v != 0;
+        else if (nm == "ws_smooth") ws_smooth = std::max(0, (int)v);
         else if (nm == "ws_policy") {
             if (v != 0 && v != 1 && v != 2) throw Failure(IFEA_INPUT_INVALID, "ws_policy: 0, 1 or 2");
             ws_policy = (int)v;
@@ -1308,6 +1484,17 @@ ifea_status ifea3d_try_update(ifea3d *ctx, double dt, int32_t *ok)
 ifea_status ifea3d_set_stream(ifea3d *ctx, void *cuda_stream)
 {
     return guarded(ctx, [&](Forging3D &s) { s.set_stream((cudaStream_t)cuda_stream); });
+}
+
+ifea_status ifea3d_set_cavity(ifea3d *ctx, int32_t n, const double *xyz)
+{
+    return guarded(ctx, [&](Forging3D &s) { s.set_cavity(n, xyz); });
+}
+
+ifea_status ifea3d_fill_percent(ifea3d *ctx, double *pct)
+{
+    if (!pct) return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) { *pct = s.fill_percent(); });
 }
 
 const char *ifea3d_last_remesh(const ifea3d *ctx) { return ctx && ctx->s ? ctx->s->last_remesh.c_str() : ""; }

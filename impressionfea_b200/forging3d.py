@@ -114,6 +114,18 @@ class Forging3DSolver:
         self._check(self._L.ifea3d_try_update(self._h, dt, C.byref(ok)))
         return bool(ok.value)
 
+    def set_cavity(self, points):
+        """Sample points of the closed cavity (meshes.cavity_samples) for fill_percent()."""
+        p = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+        self._check(self._L.ifea3d_set_cavity(self._h, len(p), _dp(p)))
+
+    def fill_percent(self):
+        """FillPercent of the snapshot (ThreeD/Forging3DSolver.cs:2174-2185): the share of the cavity samples inside
+        the current mesh, counted on the GPU."""
+        v = C.c_double()
+        self._check(self._L.ifea3d_fill_percent(self._h, C.byref(v)))
+        return v.value
+
     def set_stream(self, cuda_stream):
         """Run this context on an external CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
         self._check(self._L.ifea3d_set_stream(self._h, C.c_void_p(int(cuda_stream))))

@@ -39,6 +39,16 @@ class HeightField:
     ny: int
     h: np.ndarray
 
+    def height_at(self, x, y):
+        """Bilinear height (HeightFieldDie.HeightAt, ThreeD/HeightFieldDie.cs:100-107), clamped to the grid."""
+        fx = min(max((x - self.x0) / self.dx, 0.0), float(self.nx))
+        fy = min(max((y - self.y0) / self.dx, 0.0), float(self.ny))
+        i, j = min(int(fx), self.nx - 1), min(int(fy), self.ny - 1)
+        u, v, w = fx - i, fy - j, self.nx + 1
+        h = self.h
+        return ((1 - u) * (1 - v) * h[j * w + i] + u * (1 - v) * h[j * w + i + 1] + (1 - u) * v * h[(j + 1) * w + i]
+                + u * v * h[(j + 1) * w + i + 1])
+
     @staticmethod
     def flat(z, half_extent=100.0):
         """Flat die as one grid cell (two triangles)."""
@@ -230,3 +240,32 @@ def gear_blank_case_3d(h, R=20.0, H=50.0, dx=0.5, seed=0, jitter=0.1, stuffed=Fa
     r = np.hypot(mesh.x[:, 0], mesh.x[:, 1])
     mesh.gap0 = float(np.max(mesh.x[:, 2] - (zm + 0.5 * gear_blank_thickness(r, **profile))))
     return mesh, (bottom, top)
+
+
+def cavity_samples(dies, outline, x_max, y_max, sym_x=True, sym_y=True, x_min=None):
+    """The closed cavity's sample points for FillPercent (BuildCavitySamples, ThreeD/Forging3DSolver.cs:2157-2172):
+    a plan-view grid of spacing sqrt(area / 2500) over the part's extent, and at every grid point inside the outline
+    (outline(x, y) < 0) where the closed dies leave a gap, points spread evenly through that gap. (n, 3) array."""
+    x0 = 0.0 if sym_x else (-x_max if x_min is None else x_min)
+    y0 = 0.0 if sym_y else -y_max
+    d = np.sqrt((x_max - x0) * (y_max - y0) / 2500.0)
+    out = []
+    x = x0 + d / 2
+    while x < x_max:
+        y = y0 + d / 2
+        while y < y_max:
+            if outline(x, y) < 0:
+                zb, zt = dies[0].height_at(x, y), dies[1].height_at(x, y)
+                if zt > zb:
+                    nz = max(1, int(round((zt - zb) / d)))
+                    for k in range(nz):
+                        out.append((x, y, zb + (k + 0.5) * (zt - zb) / nz))
+            y += d
+        x += d
+    return np.array(out, np.float64).reshape(-1, 3)
+
+
+def gear_blank_outline(x, y, rim_r=45.0, flash_t=3.0, land_ratio=3.0, ramp=4.0):
+    """Plan-view outline of the gear blank's impression (negative inside): the flash land up to where the ramp to
+    the open gutter starts."""
+    return float(np.hypot(x, y)) - (rim_r + land_ratio * flash_t - 0.5 * ramp)

@@ -151,6 +151,12 @@ ifea_status ifea_spd_solve(ifea_spd *s, const double *b, double *x);
 int64_t ifea_spd_factor_nonzeros(const ifea_spd *s);
 const char *ifea_spd_name(const ifea_spd *s);
 
+/* Snapshot telemetry: FillPercent (ThreeD/Forging3DSolver.cs:2174-2185) on the device. The cavity samples
+ * (BuildCavitySamples, :2157-2172: columns over the impression between the closed dies; 3 per point) are given once;
+ * each call counts the ones inside the current mesh. The volume change is ifea3d_get_scalar(ctx, "volume"). */
+ifea_status ifea3d_set_cavity(ifea3d *ctx, int32_t n, const double *xyz);
+ifea_status ifea3d_fill_percent(ifea3d *ctx, double *pct);
+
 /* ------------------------------------------------------------------ remeshing (3D, host side)
  *
  * With ifea3d_set_scalar(ctx, "remesh", 1) the stepper remeshes where the reference does (RemeshTrigger at the

@@ -20,6 +20,10 @@ RTOL_ELEM = 1e-12      # per-element / per-node FP64 arithmetic (a few ulps of p
 RTOL_ENERGY = 1e-10    # global sums: 1/2 v.K_vol.v cancels the penalty terms, so its summation order shows
 RTOL_STATE = 1e-6      # velocity, strain and load over Newton iterations and increments
 RTOL_X = 1e-7          # coordinates after increments (moved by dt * velocity)
+# effective strain after increments: the time integral of the strain rate, a derivative of the velocity, so on
+# this coarse 1.6k-tet mesh it carries about 1.5 times the velocity's relative difference (the published meshes
+# hold it to 1e-6: tests/test_gpu_baseline_meshes.py)
+RTOL_STRAIN = 3e-6
 
 
 def _case(friction=0.3, R=10.0, H=20.0, h=2.0, shut=12.0, seed=1):
@@ -139,7 +143,7 @@ def test_increments_track_the_oracle(wide_rows):
         # x moves by dt * vg: it inherits the velocity's 1e-6 relative tolerance scaled by the stroke increment
         # over the billet size (0.2 / 20 here), so 1e-7 of the largest coordinate
         _close(gpu.array("x"), ora.array("x"), RTOL_X, f"step {k + 1}: coordinates")
-        _close_l2(gpu.array("eps"), ora.array("eps"), RTOL_STATE, f"step {k + 1}: effective strain")
+        _close_l2(gpu.array("eps"), ora.array("eps"), RTOL_STRAIN, f"step {k + 1}: effective strain")
         assert abs(gpu.scalar("gap") - ora.scalar("gap")) < 1e-12
     if wide_rows is not None:
         assert gpu.scalar("big_fronts") > 0
