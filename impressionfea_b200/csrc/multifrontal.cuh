@@ -797,7 +797,10 @@ static __global__ void __launch_bounds__(256, 2) k_update_tc(Dev<float> D, const
     if (nt <= 0) return;
     // row tiles of 128, column tiles of 64: row tile ti covers column tiles 0 .. 2 ti + 1
     int nti = (nt + tcu::TM - 1) / tcu::TM, ntiles = nti * (nti + 1);
-    if ((int)blockIdx.x >= ntiles) return;  // both exits come before the tensor memory is taken
+    // each CTA takes a contiguous run of tiles, so that consecutive tiles mostly share their row tile and the A
+    // operand (its 128 rows of the panel, split into TF32 high and low parts) is staged once per row tile
+    int chunk = (ntiles + gridDim.x - 1) / gridDim.x, t_begin = blockIdx.x * chunk, t_end = min(ntiles, t_begin + chunk);
+    if (t_begin >= ntiles) return;  // both exits come before the tensor memory is taken
     float *F = D.F + D.front_off[s];
     int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
@@ -811,7 +814,8 @@ static __global__ void __launch_bounds__(256, 2) k_update_tc(Dev<float> D, const
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::);
     uint32_t tmem = *tslot, parity = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int staged_ti = -1;
+    for (int t = t_begin; t < t_end; t++) {
         int ti = (int)((sqrt(4.0 * t + 1.0) - 1.0) * 0.5);  // row tile ti owns tiles ti (ti + 1) .. (ti + 1)(ti + 2) - 1
         while ((ti + 1) * (ti + 2) <= t) ti++;
         while (ti * (ti + 1) > t) ti--;
@@ -821,7 +825,7 @@ static __global__ void __launch_bounds__(256, 2) k_update_tc(Dev<float> D, const
         {
             // threads 0..127 stage the 128 rows of A, 128..191 the 64 rows of B (the panel's columns of each row)
             int m = tid < 128 ? tid : tid - 128;
-            if (tid < 128 + tcu::TN) {
+            if (tid < 128 + tcu::TN && (tid >= 128 || ti != staged_ti)) {
                 int row = (tid < 128 ? ri0 : cj0) + m;
                 float4 *hi = tid < 128 ? Ahi : Bhi, *lo = tid < 128 ? Alo : Blo;
                 int rows = tid < 128 ? tcu::TM : tcu::TN;
@@ -844,6 +848,7 @@ static __global__ void __launch_bounds__(256, 2) k_update_tc(Dev<float> D, const
                 }
             }
         }
+        staged_ti = ti;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {

@@ -628,6 +628,20 @@ struct Placer {
     {
         return tet_quality(x[t[4 * (size_t)e]], x[t[4 * (size_t)e + 1]], x[t[4 * (size_t)e + 2]], x[t[4 * (size_t)e + 3]]);
     }
+    // nodes of the tets below qtarget (the tets' qualities on the host's threads); false if there are none
+    bool mark_bad(const std::vector<d3> &x, double qtarget, std::vector<uint8_t> &bad) const
+    {
+        std::vector<uint8_t> low(M.ne);
+        parallel_for(M.ne, [&](int e) { low[e] = quality(x, e) < qtarget; });
+        std::fill(bad.begin(), bad.end(), 0);
+        bool any = false;
+        for (int e = 0; e < M.ne; e++) {
+            if (!low[e]) continue;
+            for (int a = 0; a < 4; a++) bad[t[4 * (size_t)e + a]] = 1;
+            any = true;
+        }
+        return any;
+    }
     double worst_around(const std::vector<d3> &x, int n) const
     {
         double q = DBL_MAX;
@@ -708,13 +722,7 @@ struct Placer {
         int moves = 0;
         std::vector<uint8_t> bad(M.nn);
         for (int s = 0; s < sweeps; s++) {
-            std::fill(bad.begin(), bad.end(), 0);
-            bool any = false;
-            for (int e = 0; e < M.ne; e++) {
-                if (quality(x, e) >= qtarget) continue;
-                for (int a = 0; a < 4; a++) bad[t[4 * (size_t)e + a]] = 1;
-                any = true;
-            }
+            bool any = mark_bad(x, qtarget, bad);
             if (!any) break;
             int sm = 0;
             for (int n = 0; n < M.nn; n++) {
@@ -759,13 +767,7 @@ struct Placer {
         int moves = 0;
         std::vector<uint8_t> bad(M.nn);
         for (int s = 0; s < sweeps; s++) {
-            std::fill(bad.begin(), bad.end(), 0);
-            bool any = false;
-            for (int e = 0; e < M.ne; e++) {
-                if (quality(x, e) >= qtarget) continue;
-                for (int a = 0; a < 4; a++) bad[t[4 * (size_t)e + a]] = 1;
-                any = true;
-            }
+            bool any = mark_bad(x, qtarget, bad);
             if (!any) break;
             int sm = 0;
             for (int n = 0; n < M.nn; n++) {

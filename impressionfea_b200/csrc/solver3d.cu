@@ -804,6 +804,18 @@ struct Forging3D {
         return sqrt(rr) <= tol * bnorm ? max_it : -1;
     }
 
+    // PCG iterations a reused factor may take. The reference's budget (PcgBudget, 15) in the FP64 form; in the
+    // single-precision form, whose factorisations are measured (device time) as are its PCG iterations (host
+    // time, syncs included), a reused factor is worth iterations up to half a factorisation's time (at least the
+    // reference's budget, at most 120)
+    int pcg_budget()
+    {
+        if (!pcg_early_abort || n_fact == 0 || lin_its == 0) return P.pcg_budget;
+        double f_ms = lin->factor_ms() / n_fact, it_ms = 1000.0 * t_pcg / lin_its;
+        if (!(f_ms > 0) || !(it_ms > 0)) return P.pcg_budget;
+        return std::max(P.pcg_budget, std::min(120, (int)(0.5 * f_ms / it_ms)));
+    }
+
     // b -> x; returns 0 for PCG, 1 for a fresh factorisation
     int solve_linear(const double *b, double *x)
     {
@@ -817,7 +829,7 @@ struct Forging3D {
             int its;
             {
                 PhaseTimer pt(t_pcg);
-                its = pcg(b, x, 1e-7, P.pcg_budget);
+                its = pcg(b, x, 1e-7, pcg_budget());
             }
             if (stale) stale_failures = its >= 0 ? 0 : stale_failures + 1;
             if (its >= 0) {
@@ -1278,6 +1290,7 @@ struct Forging3D {
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
         S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows) S("tc_updates", lin->tc_launches())
         S("factor_gflop", factor_gflop())
+        S("pcg_budget_now", pcg_budget())
         S("ws_used", ws_used) S("ws_fallbacks", ws_fallbacks) S("ws_mode", ws_mode) S("ws_policy", ws_policy) S("ws_smooth", ws_smooth)
         S("ws_last_step", ws_last_step)
         S("remesh", remesh_enabled) S("remesh_count", remesh_count) S("remesh_rejected", remesh_rejected)
