@@ -145,6 +145,11 @@ SIGNATURES = {
     "ifea3d_last_remesh": (C.c_char_p, [_vp]),
     "ifea3d_set_cavity": (_st, [_vp, C.c_int32, _dp]),
     "ifea3d_fill_percent": (_st, [_vp, _dp]),
+    "ifea_batch_create": (_st, [C.c_int32, C.POINTER(_vp), C.c_int32, C.POINTER(_vp), C.c_int32, C.POINTER(_vp)]),
+    "ifea_batch_step": (_st, [_vp, C.c_int32, C.POINTER(StepInfo), _i32p]),
+    "ifea_batch_destroy": (None, [_vp]),
+    "ifea3d_autotune": (_st, [_vp, C.c_int32, _dp, _dp, _dp]),
+    "ifea3d_time_factor_solve": (_st, [_vp, _dp]),
     "ifea_tetmesh_stuff": (_st, [INSIDE_FN, _vp, _dp, _dp, C.c_double, C.c_int32, C.c_int32, C.POINTER(_vp)]),
     "ifea_tetmesh_refine": (_st, [_vp, SIZE_FN, _vp, C.c_int32, _i32p]),
     "ifea_tetmesh_node_count": (C.c_int32, [_vp]),

@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libifea_gpu.so")
-SOURCES = ["solver3d.cu", "solver2d.cu", "spd_capi.cu", "mesh3d.cpp", "mesh2d.cpp", "multifrontal.cpp", "band_noalloc.cu", "mlp.cu", "remesh.cu"]
+SOURCES = ["solver3d.cu", "solver2d.cu", "spd_capi.cu", "mesh3d.cpp", "mesh2d.cpp", "multifrontal.cpp", "band_noalloc.cu", "mlp.cu", "remesh.cu", "batch.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

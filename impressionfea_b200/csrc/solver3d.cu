@@ -1031,6 +1031,31 @@ struct Forging3D {
         return true;
     }
 
+    // one factorisation of the current (assembled, constrained) matrix and one solve, device milliseconds: the
+    // measurement the launch-parameter tuner compares (ifea3d_autotune)
+    double time_factor_solve()
+    {
+        if (need_analyze) {
+            analyze_pattern();
+            need_analyze = false;
+        }
+        cudaEvent_t a, b;
+        cuda_check(cudaEventCreate(&a), "cudaEventCreate");
+        cuda_check(cudaEventCreate(&b), "cudaEventCreate");
+        cuda_check(cudaEventRecord(a, st), "cudaEventRecord");
+        lin->factorize(d_val);
+        lin->solve(d_r, d_dv);
+        cuda_check(cudaEventRecord(b, st), "cudaEventRecord");
+        cuda_check(cudaEventSynchronize(b), "cudaEventSynchronize");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        have_factor = true;
+        factor_step = step_index;
+        return ms;
+    }
+
     // ---------------------------------------------------------------- FillPercent (:2149-2189)
     void set_cavity(int n, const double *xyz)
     {
@@ -1497,6 +1522,12 @@ ifea_status ifea3d_try_update(ifea3d *ctx, double dt, int32_t *ok)
 ifea_status ifea3d_set_stream(ifea3d *ctx, void *cuda_stream)
 {
     return guarded(ctx, [&](Forging3D &s) { s.set_stream((cudaStream_t)cuda_stream); });
+}
+
+ifea_status ifea3d_time_factor_solve(ifea3d *ctx, double *ms)
+{
+    if (!ms) return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) { *ms = s.time_factor_solve(); });
 }
 
 ifea_status ifea3d_set_cavity(ifea3d *ctx, int32_t n, const double *xyz)

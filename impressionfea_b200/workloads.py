@@ -49,3 +49,33 @@ def closed_die_gear_blank(target_tets=200000, seed=None):
 
 def upsetting_2d():
     return Forging2DConfig()
+
+
+def batched_sweep(n_cases=64, seed=4096):
+    """Independent upsetting cases of uneven size: half 2D axisymmetric (2k-20k quads), half 3D quarter models
+    (5k-80k tets), each with its own seeded draw of aspect h/d ~ U[0.8, 2.0], friction m_f ~ U[0.1, 0.6],
+    C ~ U[80, 200] MPa, n ~ U[0, 0.2], m ~ U[0.05, 0.25]. Returns [("2d", cfg) | ("3d", cfg, mesh, dies)]."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for c in range(n_cases):
+        aspect = rng.uniform(0.8, 2.0)
+        friction, Cc, n, m = rng.uniform(0.1, 0.6), rng.uniform(80, 200), rng.uniform(0, 0.2), rng.uniform(0.05, 0.25)
+        R = 10.0
+        H = aspect * 2 * R
+        if c % 2 == 0:
+            ne = int(rng.uniform(2000, 20000))
+            nx = max(4, int(round(np.sqrt(ne * R / H))))
+            nz = max(4, int(round(ne / nx)))
+            cfg = Forging2DConfig(C=Cc, N=n, M=m, eps0=0.01, friction=friction, ram=10.0, ds=0.5 * H / 100, tol=1e-6,
+                                  radius=R, height=H, nx=nx, nz=nz,
+                                  top_profile=np.array([[0.0, 0.5 * H], [200.0, 0.5 * H]]))
+            cases.append(("2d", cfg))
+        else:
+            tets = int(rng.uniform(5000, 80000))
+            h = round(h_for_tets(R, H, tets), 3)
+            shut = 0.6 * H
+            mesh, dies = upset_case_3d(R, H, h, shut, seed=c)
+            cfg = Forging3DConfig(C=Cc, N=n, M=m, eps0=0.01, friction=friction, ram=50.0, h=h, ds=(H - shut) / 80,
+                                  size=H, tol=1e-3)
+            cases.append(("3d", cfg, mesh, dies))
+    return cases

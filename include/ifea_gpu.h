@@ -157,6 +157,27 @@ const char *ifea_spd_name(const ifea_spd *s);
 ifea_status ifea3d_set_cavity(ifea3d *ctx, int32_t n, const double *xyz);
 ifea_status ifea3d_fill_percent(ifea3d *ctx, double *pct);
 
+/* ------------------------------------------------------------------ many cases at once
+ *
+ * Independent cases (the reference: Parallel.For over the levels of a mesh study, ThreeD/MeshConvergence.cs:117)
+ * stepped together: each context keeps its own streams and graphs, a pool of host threads (threads <= 0: one per
+ * case, at most the host's hardware threads) steps them, so their kernels share the GPU. The contexts must not be
+ * used elsewhere while ifea_batch_step runs. infos: (n3 + n2) x increments, case-major (3D cases first);
+ * status: one per case (the first failure of that case; its later increments are skipped). */
+typedef struct ifea_batch ifea_batch;
+typedef struct ifea2d ifea2d;
+ifea_status ifea_batch_create(int32_t n3, ifea3d *const *ctx3, int32_t n2, ifea2d *const *ctx2, int32_t threads,
+                              ifea_batch **out);
+ifea_status ifea_batch_step(ifea_batch *b, int32_t increments, ifea_step_info *infos, int32_t *status);
+void ifea_batch_destroy(ifea_batch *b);
+/* Launch-parameter tuner: times one factorisation + solve of the next increment's first matrix for every pair of
+ * (tensor-core trailing update from 512 / 1024 / 2048 rows / never) x (multi-CTA solves from 96 / 192 / 384 rows)
+ * and keeps the fastest; with use_cache, a pair found before for the same size class (log2 of the equation count)
+ * is applied without measuring. Call after choosing the precision (factor_fp32). */
+ifea_status ifea3d_autotune(ifea3d *ctx, int32_t use_cache, double *tc_rows, double *wide_rows, double *best_ms);
+/* one factorisation of the current matrix and one solve, device milliseconds (what the tuner compares) */
+ifea_status ifea3d_time_factor_solve(ifea3d *ctx, double *ms);
+
 /* ------------------------------------------------------------------ remeshing (3D, host side)
  *
  * With ifea3d_set_scalar(ctx, "remesh", 1) the stepper remeshes where the reference does (RemeshTrigger at the
