@@ -423,6 +423,70 @@ def leg_2d(stream, threads):
             "oracle": {"increments_per_s": n_inc / t_cpu, "cores": threads, "kind": "port"}}
 
 
+def batch_leg(increments=3):
+    """64 independent upsetting cases of uneven size (32 2D axisymmetric, 2k-20k quads; 32 3D quarter models,
+    5k-80k tets): every case warmed up by one increment, then `increments` more stepped one case after another and
+    then all cases together from a pool of host threads (ForgingBatch), with and without the tuned launch
+    parameters. Wall clock around synchronised regions (the cases run on many streams)."""
+    import torch
+
+    from impressionfea_b200.batch import ForgingBatch, autotune
+    from impressionfea_b200.forging2d import ForgingSolver2D
+    from impressionfea_b200.forging3d import Forging3DSolver
+    from impressionfea_b200.workloads import batched_sweep
+
+    cases = batched_sweep()
+
+    def make(tune=False):
+        s3, s2 = [], []
+        for c in cases:
+            if c[0] == "3d":
+                s = Forging3DSolver(c[1], c[2], c[3])
+                s.set_scalar("factor_fp32", 1)
+                s3.append(s)
+            else:
+                s2.append(ForgingSolver2D(c[1]))
+        for s in s3 + s2:
+            s.step()
+        if tune:
+            for s in s3:
+                autotune(s)
+        torch.cuda.synchronize()
+        return s3, s2
+
+    out = {"workload": "64 independent upsetting cases (32 2D axisymmetric 2k-20k quads, 32 3D quarter cylinders "
+                       "5k-80k tets, seeded aspect/friction/material draws)", "increments_per_case": increments}
+    s3, s2 = make()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loads_seq = []
+    for s in s3 + s2:
+        for _ in range(increments):
+            loads_seq.append(s.step()["load"])
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    for s in s3 + s2:
+        s.close()
+    n = len(cases) * increments
+    out["sequential"] = {"case_increments_per_s": n / t_seq, "seconds": t_seq}
+    for name, tune in (("batched", False), ("batched_tuned", True)):
+        s3, s2 = make(tune)
+        b = ForgingBatch(s3, s2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        infos, status = b.step(increments)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        loads = [i["load"] for case in infos for i in case]
+        out[name] = {"case_increments_per_s": n / t, "seconds": t, "speedup_vs_sequential": t_seq / t,
+                     "failed_cases": int((status != 0).sum()),
+                     "load_rel_max_vs_sequential": float(max(abs(a / c - 1) for a, c in zip(loads, loads_seq) if c))}
+        b.close()
+        for s in s3 + s2:
+            s.close()
+    return out
+
+
 def run_gpu(args, rank, world):
     import torch
 
@@ -528,7 +592,8 @@ def run_gpu(args, rank, world):
     threads = os.cpu_count()
     if rank == 0 and not args.no_side_legs:
         for name, fn in (("upsetting_drop_in", lambda: upsetting_leg(stream, flush, W, K, 0 if args.no_cpu_baseline else 3, threads)),
-                         ("axisymmetric_2d", lambda: leg_2d(stream, threads))):
+                         ("axisymmetric_2d", lambda: leg_2d(stream, threads)),
+                         ("batched_sweep", batch_leg)):
             try:
                 legs[name] = fn()
             except Exception as e:  # reported, not fatal: the headline stands on its own

@@ -410,12 +410,7 @@ __global__ void k_read_err(int *err, int *out) { *out = *err; *err = 0; }
 template <int N, int EPI>
 void launch_gemm(const Gemm &g, int splits, cudaStream_t s)
 {
-    static bool attr = false;
-    if (!attr) {
-        cuda_check(cudaFuncSetAttribute((const void *)k_gemm<N, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem<N>()),
-                   "cudaFuncSetAttribute");
-        attr = true;
-    }
+    ensure_dynamic_smem((const void *)k_gemm<N, EPI>, gemm_smem<N>());
     dim3 grid((g.M + BM - 1) / BM, splits);
     k_gemm<N, EPI><<<grid, 128, gemm_smem<N>(), s>>>(g);
 }

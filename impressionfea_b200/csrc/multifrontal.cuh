@@ -1262,7 +1262,7 @@ public:
         wide_smem_ = 8;
         for (int sn : big_list_) wide_smem_ = std::max(wide_smem_, (size_t)std::max(S.ncol[sn], S.m[sn] - S.ncol[sn]) * sizeof(T));
         if (wide_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the wide solve kernels' shared-memory window");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_wide_bwd_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wide_smem_), "cudaFuncSetAttribute");
+        ensure_dynamic_smem((const void *)mf::k_wide_bwd_x<T>, (int)wide_smem_);
         // inverse passes of the wide supernodes, per level: diagonal copies, then for groups of 2, 4, ... blocks
         // the T pass and the X21 pass, each followed by its reduction when a block range was split
         std::vector<mf::XTask> tasks;
@@ -1336,23 +1336,17 @@ public:
         dev_.gat_start = d_gst_; dev_.gat_src = d_gsrc_;
         dev_.inv_off = d_inv_off_; dev_.Inv = d_Inv_; dev_.xinv_off = d_xinv_off_; dev_.Xinv = d_Xinv_;
         dev_.Abig = d_Abig_;
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kUpdateSmem), "cudaFuncSetAttribute");
+        ensure_dynamic_smem((const void *)mf::k_update<T>, (int)kUpdateSmem);
         if constexpr (std::is_same<T, float>::value)
-            cuda_check(cudaFuncSetAttribute((const void *)mf::k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            mf::tcu::kSmem), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kPanelSmem), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_panel_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kPairSmem), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_xinv_gemm<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kPairSmem), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_xinv_gemm<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kPairSmem), "cudaFuncSetAttribute");
+            ensure_dynamic_smem((const void *)mf::k_update_tc, mf::tcu::kSmem);
+        ensure_dynamic_smem((const void *)mf::k_panel<T>, (int)kPanelSmem);
+        ensure_dynamic_smem((const void *)mf::k_panel_trsm<T>, (int)kPairSmem);
+        ensure_dynamic_smem((const void *)mf::k_xinv_gemm<T, 0>, (int)kPairSmem);
+        ensure_dynamic_smem((const void *)mf::k_xinv_gemm<T, 1>, (int)kPairSmem);
         if (small_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the solve kernels' shared-memory window");
         level_smem_ = std::max(small_smem_, wide_smem_);
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_fwd_level<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_smem_), "cudaFuncSetAttribute");
-        cuda_check(cudaFuncSetAttribute((const void *)mf::k_bwd_level<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)level_smem_), "cudaFuncSetAttribute");
+        ensure_dynamic_smem((const void *)mf::k_fwd_level<T>, (int)small_smem_);
+        ensure_dynamic_smem((const void *)mf::k_bwd_level<T>, (int)level_smem_);
         cuda_check(cudaStreamSynchronize(st_), "cudaStreamSynchronize");
         analyzed_ = true;
     }

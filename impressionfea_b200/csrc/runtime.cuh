@@ -4,6 +4,8 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -26,6 +28,22 @@ struct CudaFailure : Failure {
 inline void cuda_check(cudaError_t e, const char *what)
 {
     if (e != cudaSuccess) throw CudaFailure(what, e);
+}
+
+// Raise a kernel's dynamic shared-memory limit on the current device to at least `bytes`. The limit belongs to the
+// kernel, not to a context: a context that needs less must not lower what another live context's launches rely on,
+// and contexts are set up from several host threads at once, hence a monotone maximum under a lock.
+inline void ensure_dynamic_smem(const void *kernel, size_t bytes)
+{
+    static std::mutex m;
+    static std::map<std::pair<const void *, int>, size_t> done;
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(m);
+    size_t &cur = done[{kernel, dev}];
+    if (bytes <= cur) return;
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), "cudaFuncSetAttribute");
+    cur = bytes;
 }
 
 // Owning device buffer (cudaMalloc / cudaFree; contents undefined after resize).

@@ -893,8 +893,7 @@ struct Forging2D {
         hs.resize(T_COUNT + 4);
         hi.resize(8);
         win_rows = band_window(nd, topo.half_band, &win_bytes);
-        cuda_check(cudaFuncSetAttribute((const void *)k_band_factor_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)win_bytes), "cudaFuncSetAttribute");
+        ensure_dynamic_smem((const void *)k_band_factor_solve, (int)win_bytes);
         // initial contact on the boundary loop (tol 1e-3 h) and velocity field (:130-139)
         View2 V = view();
         k2_init_contact<<<grid(topo.nloop), 128, 0, st>>>(V, 1e-3 * h);
@@ -1374,8 +1373,7 @@ ifea_status ifea_band_factor_solve(int32_t n, int32_t half_bandwidth, double *ba
         err.resize(1);
         size_t bytes = 0;
         int W = ifea::band_window(n, b, &bytes);
-        ifea::cuda_check(cudaFuncSetAttribute((const void *)ifea::k_band_factor_solve,
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), "cudaFuncSetAttribute");
+        ifea::ensure_dynamic_smem((const void *)ifea::k_band_factor_solve, (int)bytes);
         ifea::k_band_factor_solve<<<1, 1024, bytes, st>>>(n, b, a, rhs ? x.p : nullptr, W, err, piv);
         ifea::cuda_check(cudaGetLastError(), "band launch");
         int32_t e = -1;

@@ -546,7 +546,7 @@ struct Forging3D {
         col_smem = per_warp * wpb;
         if (per_warp > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "node neighbourhood too large for the column kernel");
         auto set_smem = [&](const void *f) {
-            cuda_check(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem), "cudaFuncSetAttribute");
+            ensure_dynamic_smem(f, (int)col_smem);
         };
         set_smem((const void *)k_columns<ASM_MATRIX, true>);
         set_smem((const void *)k_columns<ASM_MATRIX, false>);
