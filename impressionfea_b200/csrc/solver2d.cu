@@ -4,9 +4,9 @@
 // Per Newton iteration: one thread per quad computes the element stiffness and residual (2x2 Gauss deviatoric
 // power + 1-point volumetric penalty, nodal (t, n) rotation); band cells and residual entries are then gathered in
 // element order (the reference's serial scatter order); fixed DOFs, friction and the band Cholesky follow. The
-// band Cholesky runs in one CTA: right-looking column sweeps over a circular window of rows held in shared
-// memory, which subtract the products in the same order as the reference's row-oriented loop, so the factor is
-// bit-identical to SymmetricBandMatrix.Factorize.
+// band Cholesky (band.cuh) runs in one CTA, blocked by panels over a circular window of rows in shared memory;
+// every entry's products are subtracted in the same order as the reference's row-oriented loop, so the factor and
+// the solution are bit-identical to SymmetricBandMatrix.Factorize / Solve.
 #include <climits>
 #include <cmath>
 #include <cstdarg>
@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "band.cuh"
 #include "common.cuh"
 #include "mesh2d.h"
 #include "runtime.cuh"
@@ -421,101 +422,6 @@ __global__ void k2_constrain(View2 V)
     }
 }
 
-}  // namespace
-
-// Band Cholesky factorisation and solve in one CTA (see the file comment). Window: W rows of (b+1) doubles in
-// shared memory, circular in the row index. err_row[0] = -1 on success, else the failing row; pivot[0] its pivot.
-__global__ void k_band_factor_solve(int n, int b, double *__restrict__ a, double *__restrict__ rhs, int W,
-                                    int32_t *err_row, double *pivot)
-{
-    extern __shared__ double win[];
-    __shared__ int s_bad;
-    const int w = b + 1;
-    int tid = threadIdx.x, nt = blockDim.x;
-    if (tid == 0) s_bad = -1;
-    // rows [0, min(n, W)) into the window
-    for (int64_t t = tid; t < (int64_t)min(n, W) * w; t += nt) win[t] = a[t];
-    __syncthreads();
-    int loaded = min(n, W);  // rows [0, loaded) have been loaded
-    for (int k = 0; k < n; k++) {
-        double *rk = win + (size_t)(k % W) * w;
-        if (tid == 0) {
-            double s = rk[b];
-            if (!(s > 0) || isnan(s)) {
-                s_bad = k;
-                *pivot = s;
-            } else {
-                rk[b] = sqrt(s);
-            }
-        }
-        __syncthreads();
-        if (s_bad >= 0) break;
-        double lkk = rk[b];
-        int imax = min(n - 1, k + b);
-        // L_ik = a_ik / L_kk
-        for (int i = k + 1 + tid; i <= imax; i += nt) win[(size_t)(i % W) * w + (k - i + b)] /= lkk;
-        __syncthreads();
-        // a_ij -= L_ik L_jk for k < j <= i <= k + b
-        int m = imax - k;  // rows below the pivot
-        int pairs = m * (m + 1) / 2;
-        for (int t = tid; t < pairs; t += nt) {
-            int di = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-            while ((di + 1) * (di + 2) / 2 <= t) di++;
-            while (di * (di + 1) / 2 > t) di--;
-            int dj = t - di * (di + 1) / 2;
-            int i = k + 1 + di, j = k + 1 + dj;
-            double lik = win[(size_t)(i % W) * w + (k - i + b)];
-            double ljk = win[(size_t)(j % W) * w + (k - j + b)];
-            win[(size_t)(i % W) * w + (j - i + b)] -= lik * ljk;
-        }
-        __syncthreads();
-        // row k is final: write it back and load the next row into its slot
-        for (int t = tid; t < w; t += nt) a[(size_t)k * w + t] = rk[t];
-        __syncthreads();
-        if (loaded < n) {
-            double *dst = win + (size_t)(loaded % W) * w;
-            for (int t = tid; t < w; t += nt) dst[t] = a[(size_t)loaded * w + t];
-            loaded++;
-        }
-        __syncthreads();
-    }
-    if (s_bad >= 0) {
-        if (tid == 0) *err_row = s_bad;
-        return;
-    }
-    if (tid == 0) *err_row = -1;
-    if (!rhs) return;
-    __syncthreads();
-    // forward: x_k = rhs_k / L_kk; rhs_i -= L_ik x_k (ascending k, as the reference's row loop)
-    for (int k = 0; k < n; k++) {
-        double xk = rhs[k] / a[(size_t)k * w + b];
-        __syncthreads();
-        if (tid == 0) rhs[k] = xk;
-        int imax = min(n - 1, k + b);
-        for (int i = k + 1 + tid; i <= imax; i += nt) rhs[i] -= a[(size_t)i * w + (k - i + b)] * xk;
-        __syncthreads();
-    }
-    // backward (SymmetricBandMatrix.cs:104-110)
-    for (int i = n - 1; i >= 0; i--) {
-        double xi = rhs[i] / a[(size_t)i * w + b];
-        __syncthreads();
-        if (tid == 0) rhs[i] = xi;
-        for (int k = max(0, i - b) + tid; k < i; k += nt) rhs[k] -= a[(size_t)i * w + (k - i + b)] * xi;
-        __syncthreads();
-    }
-}
-
-namespace {
-
-// Window rows that fit the shared memory budget (at least b + 1).
-int band_window(int n, int b, size_t *bytes)
-{
-    size_t per_row = (size_t)(b + 1) * sizeof(double);
-    int W = (int)std::min<size_t>((size_t)n, std::max<size_t>((size_t)b + 1, (200 * 1024) / per_row));
-    *bytes = (size_t)W * per_row;
-    return W;
-}
-
 __global__ void k2_frames(View2 V)
 {
     GS2(n, V.nn)
@@ -816,8 +722,7 @@ struct Forging2D {
     int vcur = 0;
     HostPinned<double> hs;
     HostPinned<int32_t> hi;
-    size_t win_bytes = 0;
-    int win_rows = 0;
+    band::Plan bplan;
 
     Forging2D(const ifea2d_params &p, int nb, const double *bxy, int ntp, const double *txy) : P(p)
     {
@@ -892,8 +797,8 @@ struct Forging2D {
         d_elsig.upload(sig, st);
         hs.resize(T_COUNT + 4);
         hi.resize(8);
-        win_rows = band_window(nd, topo.half_band, &win_bytes);
-        ensure_dynamic_smem((const void *)k_band_factor_solve, (int)win_bytes);
+        bplan = band::plan(nd, topo.half_band);
+        ensure_dynamic_smem(band::kernel_of(bplan), bplan.bytes);
         // initial contact on the boundary loop (tol 1e-3 h) and velocity field (:130-139)
         View2 V = view();
         k2_init_contact<<<grid(topo.nloop), 128, 0, st>>>(V, 1e-3 * h);
@@ -1005,7 +910,7 @@ struct Forging2D {
     void factor_solve(double *rhs)
     {
         cuda_check(cudaMemsetAsync(d_err.p + 2, 0xff, sizeof(int32_t), st), "memset");
-        k_band_factor_solve<<<1, 1024, win_bytes, st>>>(topo.ndof, topo.half_band, d_band, rhs, win_rows, d_err.p + 2, d_piv);
+        band::launch(bplan, topo.ndof, topo.half_band, d_band, rhs, d_err.p + 2, d_piv, st);
         cuda_check(cudaGetLastError(), "band factor launch");
         int32_t e4[4];
         read_err(e4);
@@ -1371,10 +1276,9 @@ ifea_status ifea_band_factor_solve(int32_t n, int32_t half_bandwidth, double *ba
         if (rhs) x.upload(rhs, n, st);
         piv.resize(1);
         err.resize(1);
-        size_t bytes = 0;
-        int W = ifea::band_window(n, b, &bytes);
-        ifea::ensure_dynamic_smem((const void *)ifea::k_band_factor_solve, (int)bytes);
-        ifea::k_band_factor_solve<<<1, 1024, bytes, st>>>(n, b, a, rhs ? x.p : nullptr, W, err, piv);
+        ifea::band::Plan plan = ifea::band::plan(n, b);
+        ifea::ensure_dynamic_smem(ifea::band::kernel_of(plan), plan.bytes);
+        ifea::band::launch(plan, n, b, a, rhs ? x.p : nullptr, err, piv, st);
         ifea::cuda_check(cudaGetLastError(), "band launch");
         int32_t e = -1;
         double pv = 0;

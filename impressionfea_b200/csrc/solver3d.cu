@@ -291,6 +291,7 @@ struct Forging3D {
     bool remesh_enabled = false;
     int remesh_count = 0, remesh_rejected = 0, refinement_levels = 1, max_nodes = 1 << 30;
     double t_remesh = 0;
+    double t_rm_stuff = 0, t_rm_refine = 0, t_rm_place = 0, t_rm_remap = 0, t_rm_setmesh = 0;  // remesh phases
     std::vector<HotSpot> hot;        // places where increments failed (later remeshes refine there)
     d3 fail_at = mk3(0, 0, 0);
     bool have_fail_at = false;
@@ -1125,7 +1126,12 @@ struct Forging3D {
             last_remesh = reason + " rejected: " + out.why;
             return false;
         }
+        t_rm_stuff += out.t_stuff;
+        t_rm_refine += out.t_refine;
+        t_rm_place += out.t_place;
+        t_rm_remap += out.t_remap;
         int nn2 = (int)(out.x.size() / 3), ne2 = (int)(out.tets.size() / 4);
+        PhaseTimer pm(t_rm_setmesh);
         set_mesh(nn2, ne2, out.x.data(), out.tets.data(), out.on_x0.data(), out.on_y0.data());
         d_vg.upload(out.vg, st);
         d_eps.upload(out.eps, st);
@@ -1319,7 +1325,7 @@ struct Forging3D {
         S("ws_used", ws_used) S("ws_fallbacks", ws_fallbacks) S("ws_mode", ws_mode) S("ws_policy", ws_policy) S("ws_smooth", ws_smooth)
         S("ws_last_step", ws_last_step)
         S("remesh", remesh_enabled) S("remesh_count", remesh_count) S("remesh_rejected", remesh_rejected)
-        S("t_remesh", t_remesh) S("refinement_levels", refinement_levels) S("max_nodes", max_nodes) S("hot_spots", hot.size())
+        S("t_remesh", t_remesh) S("t_rm_stuff", t_rm_stuff) S("t_rm_refine", t_rm_refine) S("t_rm_place", t_rm_place) S("t_rm_remap", t_rm_remap) S("t_rm_setmesh", t_rm_setmesh) S("refinement_levels", refinement_levels) S("max_nodes", max_nodes) S("hot_spots", hot.size())
 #undef S
         if (nm == "volume") return volume();
         if (nm == "fill_percent") return fill_percent();

@@ -313,12 +313,12 @@ ifea_status ifea_band_factor_solve(int32_t n, int32_t half_bandwidth, double *ba
  * pooling allocator, or the solve sits in a loop that must not call cudaMalloc/cudaFree). d_band (n*(b+1) doubles,
  * the same row-wise lower band as ifea_band_factor_solve) is overwritten by L, d_rhs (n doubles, may be NULL) by x;
  * work is issued on cuda_stream (a cudaStream_t, NULL = default stream) and the call returns after it finished.
- * The only working memory is a fixed 2 MiB device array inside the library, present on every GPU that loads it
- * until the process exits: half-bandwidths above 510 are rejected with IFEA_INPUT_INVALID. Every call looks up
- * that array's device address in the current device's context, launches one kernel, copies the two status words
- * back and waits for cuda_stream to finish. All calls on a device share the array and it keeps the last call's
- * contents; each call re-initialises what it reads (window and status words), but calls that overlap on the same
- * GPU race on it and must be serialised by the caller.
+ * The factorisation's working rows live in the kernel's shared memory, or, for a band too wide for that window,
+ * in d_band itself; the only other working memory is a fixed 16-byte device array inside the library holding the
+ * two status words, present on every GPU that loads it until the process exits. Every call looks up that array's
+ * device address in the current device's context, launches one kernel, copies the status words back and waits
+ * for cuda_stream to finish. All calls on a device share the status words; each call re-initialises them, but
+ * calls that overlap on the same GPU race on them and must be serialised by the caller.
  * Returns IFEA_NOT_SPD with *bad_row / *pivot on a non-positive pivot. Allocates nothing. */
 ifea_status ifea_band_factor_solve_noalloc(int32_t n, int32_t half_bandwidth, double *d_band, double *d_rhs,
                                            int32_t *bad_row, double *pivot, void *cuda_stream);

@@ -337,6 +337,15 @@ class OracleBand:
         ptr = self.L.oband_data(self.h, C.byref(n))
         return _view(ptr, n.value, np.float64)
 
+    def set_data(self, a):
+        """Overwrite the stored band (row-wise lower band, n * (b + 1) values) in one copy."""
+        n = C.c_int64()
+        ptr = self.L.oband_data(self.h, C.byref(n))
+        a = np.ascontiguousarray(a, np.float64)
+        if a.size != n.value:
+            raise ValueError(f"band of {a.size} values, the matrix stores {n.value}")
+        C.memmove(ptr, a.ctypes.data, a.nbytes)
+
     def close(self):
         if self.h:
             self.L.oband_destroy(self.h)

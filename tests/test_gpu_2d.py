@@ -79,6 +79,43 @@ def test_gpu_band_cholesky_is_bit_identical_to_the_reference_loop():
     np.testing.assert_array_equal(x, x_ref)
 
 
+def _spd_band(n, b, seed):
+    rng = np.random.default_rng(seed)
+    w = b + 1
+    a = np.zeros(n * w)
+    for i in range(n):
+        lo = max(0, i - b)
+        a[i * w + (lo - i + b):i * w + b] = rng.random(i - lo) - 0.5
+        a[i * w + b] = 2.0 * b + 1.0 + rng.random()
+    return a, rng.standard_normal(n)
+
+
+# (n, half-bandwidth): bands narrower than a panel (1, 5), one column either side of the 32-column panel, a
+# circular window reloaded many times (2000 x 85: the 2D decks' shape; 3000 x 60), the whole band resident
+# (90 x 64, 70 x 69, 150 x 110), 16- and 8-column panels (1200 x 140, 1200 x 145) and a band too wide for the
+# shared-memory window, factorised in place (1500 x 160)
+@pytest.mark.parametrize("n,b", [(100, 1), (200, 5), (150, 31), (150, 33), (2000, 85), (3000, 60), (90, 64),
+                                 (70, 69), (150, 110), (1200, 140), (1200, 145), (1500, 160)])
+def test_blocked_band_cholesky_is_bit_identical_to_the_reference_loop(n, b):
+    a, rhs = _spd_band(n, b, n + b)
+    ob = OracleBand(n, b)
+    ob.set_data(a)
+    row, _ = ob.factorize()
+    assert row == -1
+    x_ref = ob.solve(rhs)
+    L, x = band_factor_solve(a, b, rhs)
+    np.testing.assert_array_equal(L, ob.data())
+    np.testing.assert_array_equal(x, x_ref)
+
+
+def test_blocked_band_reports_the_first_failing_row_inside_a_panel():
+    n, b = 400, 40
+    a, rhs = _spd_band(n, b, 5)
+    a[77 * (b + 1) + b] = -3.0  # row 77: the third panel's 14th column
+    with pytest.raises(_lib.MatrixNotPositiveDefiniteError, match="equation 77 "):
+        band_factor_solve(a, b, rhs)
+
+
 def test_gpu_band_reports_non_positive_pivot():
     # NumericsTests.cs:40-48
     a = np.zeros(3 * 2)

@@ -1,15 +1,17 @@
 """The no-allocation band entry point (ifea_band_factor_solve_noalloc) against the allocating one.
 
 Callers whose device memory is owned by their own pooling allocator, or that run a solve inside a loop where
-cudaMalloc/cudaFree must not happen, hand in device buffers they already own; the entry point's only working
-memory is a fixed device array inside the library, shared by every call on a GPU and never cleared between them.
-These tests call it through the C ABI several times in a row and compare each result with ifea_band_factor_solve
-on the same system, bit for bit (both kernels subtract the products in the same order):
+cudaMalloc/cudaFree must not happen, hand in device buffers they already own; the entry point's working rows sit
+in shared memory (or, for a band too wide for that window, in the caller's band) and its status words in a fixed
+device array inside the library, shared by every call on a GPU and never cleared between them. These tests call
+it through the C ABI several times in a row and compare each result bit for bit with ifea_band_factor_solve on the
+same system, or with the reference's band loop (oracle):
 
-- two successful calls in a row, the first with a half-bandwidth wide enough that only part of the band fits the
-  fixed array at once (the circular row window is reloaded as the factorisation walks down the band);
+- three successful calls in a row: a band factorised in place (too wide for the shared-memory window), a band
+  whose circular window is reloaded as the factorisation walks down it, and a band resident as a whole;
 - a call that fails on a non-positive pivot followed by a good call, so that the failed call's status words,
-  which stay in the array, must not leak into the next result.
+  which stay in the array, must not leak into the next result;
+- a half-bandwidth of 511 (wider than any shared-memory window), against the reference loop.
 """
 import ctypes as C
 
@@ -18,11 +20,9 @@ import pytest
 
 from impressionfea_b200 import _lib
 from impressionfea_b200.forging2d import band_factor_solve
+from oracle import OracleBand
 
 pytestmark = pytest.mark.gpu
-
-SCRATCH_DOUBLES = 262144 - 32  # row window capacity of the fixed array, in doubles
-
 
 def _spd_band(n, b, seed):
     rng = np.random.default_rng(seed)
@@ -59,12 +59,10 @@ def _check_against_allocating_entry(n, b, seed, label):
     np.testing.assert_array_equal(x_gpu, x_ref, err_msg=label)
 
 
-def test_noalloc_matches_allocating_entry_on_two_calls_in_a_row():
-    # n = 3000, b = 160: the window holds 262112 // 161 = 1628 rows < n, so rows are reloaded into its slots
-    # (b = 160 also keeps the allocating entry point's shared-memory window, 161 rows of 161 doubles, in bounds).
-    assert SCRATCH_DOUBLES // 161 < 3000
-    _check_against_allocating_entry(3000, 160, 11, "call 1 (circular window)")
-    _check_against_allocating_entry(400, 40, 12, "call 2 (whole band in the window)")
+def test_noalloc_matches_allocating_entry_on_calls_in_a_row():
+    _check_against_allocating_entry(3000, 160, 11, "call 1 (in place: 162-double rows do not fit the window)")
+    _check_against_allocating_entry(3000, 60, 14, "call 2 (circular window of 124 rows, reloaded)")
+    _check_against_allocating_entry(400, 40, 12, "call 3 (whole band in the window)")
 
 
 def test_noalloc_good_call_after_a_failed_one_reports_no_stale_status():
@@ -75,7 +73,14 @@ def test_noalloc_good_call_after_a_failed_one_reports_no_stale_status():
     _check_against_allocating_entry(900, 85, 13, "good call after a NOT_SPD call")
 
 
-def test_noalloc_rejects_a_band_wider_than_the_fixed_array():
-    n, b = 600, 511  # (b + 1)^2 doubles exceed the fixed scratch array
-    st, _, _, _, _ = _noalloc(np.ones(n * (b + 1)), np.ones(n), b)
-    assert st == 1
+def test_noalloc_wide_band_matches_the_reference_loop():
+    n, b = 600, 511
+    a, rhs = _spd_band(n, b, 15)
+    ob = OracleBand(n, b)
+    ob.set_data(a)
+    assert ob.factorize()[0] == -1
+    x_ref = ob.solve(rhs)
+    st, row, _, L_gpu, x_gpu = _noalloc(a, rhs, b)
+    assert st == 0 and row == -1
+    np.testing.assert_array_equal(L_gpu, ob.data())
+    np.testing.assert_array_equal(x_gpu, x_ref)
