@@ -6,8 +6,9 @@
 // in ascending k (forward) and descending i (backward). Any schedule that keeps that order per entry gives the
 // same bits, so the factorisation here is blocked by panels of nb columns:
 //
-//   A  panel factorisation: column by column inside the panel (pivot, scale, update of the panel's later
-//      columns), all threads, two barriers per column;
+//   A  panel factorisation: column by column inside the panel (scale, update of the panel's later columns,
+//      pivot), the panel's entries held in registers (each thread some rows of one column), two barriers per
+//      column;
 //   B  trailing update of the rows below the panel by the whole panel: 4 x 4 register tiles, each entry's nb
 //      products subtracted in ascending k (one shared-memory load per two multiplies);
 //   C  the forward substitution of the panel's rows and its update of the b rows below, by one warp, while the
@@ -31,6 +32,8 @@ namespace band {
 
 constexpr int kThreads = 512;
 constexpr int kMaxSmem = 200 * 1024;
+constexpr int kOwn = 10;          // panel entries a thread keeps in registers
+constexpr int kStageRows = 256;   // panel rows the register path takes
 
 struct Plan {
     int nb = 32, W = 0;
@@ -79,6 +82,7 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
     extern __shared__ __align__(16) unsigned char band_smem[];
     __shared__ int s_bad;
     __shared__ double xs[32];
+    __shared__ double lcol[kStageRows], stage[kStageRows];  // the scaled column kk; the updated column kk + 1
     const int w = b + 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned FULL = 0xffffffffu;
@@ -161,24 +165,76 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
         if (s_bad >= 0) break;
         auto P = [&](int i, int j) -> double & { return win[rowoff[i - k0] + j]; };
 
-        // A: the panel's columns
-        for (int k = k0; k < k1; k++) {
-            const double lkk = P(k, k);
-            const int r = min(n - 1, k + b);
-            for (int i = k + 1 + tid; i <= r; i += kThreads) P(i, k) = P(i, k) / lkk;
-            __syncthreads();
-            const int c = k1 - 1 - k, rows = r - k;
-            for (int idx = tid; idx < c * rows; idx += kThreads) {
-                int di = idx / c, dj = idx - di * c;
-                int i = k + 1 + di, j = k + 1 + dj;
-                if (j <= i) {
-                    double &e = P(i, j);
-                    e = e - P(i, k) * P(j, k);
-                    if (idx == 0) do_pivot(k + 1);  // (k + 1, k + 1) is final now
-                }
+        // A: the panel's columns. Rows r = 0 .. R - 1 of the panel (relative to k0); with the window in shared
+        // memory and at most kOwn rows per thread, every thread keeps the entries of one panel column (ct) in
+        // registers, rows rt, rt + step, ..., and a column step is: scale column kk (one row per thread, into
+        // the window and lcol), barrier, each thread subtracts column kk's products from its entries (the owners
+        // of column kk + 1 then hand it to stage[] and its pivot is taken), barrier.
+        const int np = k1 - k0, R = last - k0 + 1;
+        const int lg = nb == 32 ? 5 : nb == 16 ? 4 : 3, step = kThreads >> lg;
+        if (SMEM && R <= kStageRows && (R + step - 1) / step <= kOwn && (1 << lg) == nb) {
+            const int ct = tid & (nb - 1), rt = tid >> lg;
+            double v[kOwn];
+#pragma unroll
+            for (int u = 0; u < kOwn; u++) {
+                int r = rt + u * step;
+                v[u] = (r < R && ct < np && r >= ct && r - ct <= b) ? P(k0 + r, k0 + ct) : 0.0;
             }
-            __syncthreads();
-            if (s_bad >= 0) break;
+            for (int kk = 0; kk < np; kk++) {
+                const int k = k0 + kk;
+                const double lkk = P(k, k);
+                for (int r = tid; r < R; r += kThreads)
+                    if (r > kk && r - kk <= b) {
+                        double l = (kk == 0 ? P(k0 + r, k) : stage[r]) / lkk;
+                        lcol[r] = l;
+                        P(k0 + r, k) = l;
+                    }
+                __syncthreads();
+                if (ct > kk && ct < np) {
+                    const double ljk = lcol[ct];
+#pragma unroll
+                    for (int u = 0; u < kOwn; u++) {
+                        int r = rt + u * step;
+                        if (r < R && r >= ct && r <= kk + b) v[u] = v[u] - lcol[r] * ljk;
+                    }
+                    if (ct == kk + 1) {
+#pragma unroll
+                        for (int u = 0; u < kOwn; u++) {
+                            int r = rt + u * step;
+                            if (r < R && r >= ct && r - ct <= b) {
+                                if (r == ct) {
+                                    P(k0 + r, k0 + r) = v[u];
+                                    do_pivot(k0 + r);  // (kk + 1, kk + 1) is final now
+                                } else {
+                                    stage[r] = v[u];
+                                }
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+                if (s_bad >= 0) break;
+            }
+        } else {
+            // column by column with every entry in the window (bands too wide for the register path)
+            for (int k = k0; k < k1; k++) {
+                const double lkk = P(k, k);
+                const int r = min(n - 1, k + b);
+                for (int i = k + 1 + tid; i <= r; i += kThreads) P(i, k) = P(i, k) / lkk;
+                __syncthreads();
+                const int c = k1 - 1 - k, rows = r - k;
+                for (int idx = tid; idx < c * rows; idx += kThreads) {
+                    int di = idx / c, dj = idx - di * c;
+                    int i = k + 1 + di, j = k + 1 + dj;
+                    if (j <= i) {
+                        double &e = P(i, j);
+                        e = e - P(i, k) * P(j, k);
+                        if (idx == 0) do_pivot(k + 1);  // (k + 1, k + 1) is final now
+                    }
+                }
+                __syncthreads();
+                if (s_bad >= 0) break;
+            }
         }
         if (s_bad >= 0) break;
 

@@ -281,6 +281,7 @@ struct Forging3D {
     // from an earlier increment again only now and then once that failed (on with the single-precision factor;
     // off in the reference's FP64 form, whose iteration counts it must reproduce)
     bool pcg_early_abort = false;
+    double pcg_budget_scale = 2.0;  // factorisations' worth of PCG iterations a reused factor may take
     int factor_step = -1, stale_failures = 0;  // increment of the cached factor; failed tries of a stale one
     int wide_rows = mf::kWideM;  // fronts at least this tall use the multi-CTA solve path
     // learned warm start: mode bit 1 records (inputs, target) of every accepted increment into the network's
@@ -807,14 +808,14 @@ struct Forging3D {
 
     // PCG iterations a reused factor may take. The reference's budget (PcgBudget, 15) in the FP64 form; in the
     // single-precision form, whose factorisations are measured (device time) as are its PCG iterations (host
-    // time, syncs included), a reused factor is worth iterations up to half a factorisation's time (at least the
-    // reference's budget, at most 120)
+    // time, syncs included), a reused factor is worth iterations up to pcg_budget_scale factorisations' time
+    // (at least the reference's budget, at most 120)
     int pcg_budget()
     {
         if (!pcg_early_abort || n_fact == 0 || lin_its == 0) return P.pcg_budget;
         double f_ms = lin->factor_ms() / n_fact, it_ms = 1000.0 * t_pcg / lin_its;
         if (!(f_ms > 0) || !(it_ms > 0)) return P.pcg_budget;
-        return std::max(P.pcg_budget, std::min(120, (int)(0.5 * f_ms / it_ms)));
+        return std::max(P.pcg_budget, std::min(120, (int)(pcg_budget_scale * f_ms / it_ms)));
     }
 
     // b -> x; returns 0 for PCG, 1 for a fresh factorisation
@@ -1321,7 +1322,7 @@ struct Forging3D {
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
         S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows) S("tc_updates", lin->tc_launches())
         S("factor_gflop", factor_gflop())
-        S("pcg_budget_now", pcg_budget())
+        S("pcg_budget_now", pcg_budget()) S("pcg_budget_scale", pcg_budget_scale)
         S("ws_used", ws_used) S("ws_fallbacks", ws_fallbacks) S("ws_mode", ws_mode) S("ws_policy", ws_policy) S("ws_smooth", ws_smooth)
         S("ws_last_step", ws_last_step)
         S("remesh", remesh_enabled) S("remesh_count", remesh_count) S("remesh_rejected", remesh_rejected)
@@ -1350,6 +1351,10 @@ struct Forging3D {
             use_precision(v != 0);
             pcg_early_abort = v != 0;
         } else if (nm == "pcg_early_abort") pcg_early_abort = v != 0;
+        else if (nm == "pcg_budget_scale") {
+            if (!(v > 0 && v <= 16)) throw Failure(IFEA_INPUT_INVALID, "pcg_budget_scale must lie in (0, 16]");
+            pcg_budget_scale = v;
+        }
         else if (nm == "remesh") remesh_enabled = v != 0;
         else if (nm == "ws_smooth") ws_smooth = std::max(0, (int)v);
         else if (nm == "ws_policy") {
