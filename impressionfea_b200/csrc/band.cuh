@@ -33,6 +33,7 @@ namespace band {
 constexpr int kThreads = 512;
 constexpr int kMaxSmem = 200 * 1024;
 constexpr int kOwn = 10;          // panel entries a thread keeps in registers
+constexpr int kBlkRows = 4;       // rows of 32 per lane in the eight-column block factorisation
 constexpr int kStageRows = 256;   // panel rows the register path takes
 
 struct Plan {
@@ -41,15 +42,16 @@ struct Plan {
     size_t bytes = 0;  // dynamic shared memory of the launch
 };
 
-// Panel width and window for an n x n band of half-bandwidth b. Window W = 2 nb + b rows of b + 1 doubles and their
-// right-hand-side entries; widest panel that fits, else the band stays in global memory (window = the band).
+// Panel width and window for an n x n band of half-bandwidth b. Window W = 2 nb + b rows of b + 1 doubles (padded
+// to an odd count) and their right-hand-side entries; widest panel that fits, else the band stays in global
+// memory (window = the band).
 inline Plan plan(int n, int b)
 {
     Plan p;
     size_t w = (size_t)b + 1;
     for (int nb : {32, 16, 8}) {
         int W = (int)std::min<int64_t>((int64_t)n, 2 * (int64_t)nb + b);
-        size_t bytes = (size_t)W * (w + 1) * sizeof(double) + (size_t)(2 * nb + b) * sizeof(int64_t);
+        size_t bytes = (size_t)W * ((w | 1) + 1) * sizeof(double) + (size_t)(2 * nb + b) * sizeof(int64_t);
         if (bytes <= (size_t)kMaxSmem) {
             p.nb = nb;
             p.W = W;
@@ -83,7 +85,11 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
     __shared__ int s_bad;
     __shared__ double xs[32];
     __shared__ double lcol[kStageRows], stage[kStageRows];  // the scaled column kk; the updated column kk + 1
+    __shared__ typename std::conditional<SMEM, int, int64_t>::type brow[32];  // row offsets of a backward block
     const int w = b + 1;
+    // window rows are an odd number of doubles apart, so that a warp reading one column of consecutive rows
+    // touches distinct banks (the band in global memory keeps its stride w)
+    const int ws = SMEM ? (w | 1) : w;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned FULL = 0xffffffffu;
     // layout: row-offset table (2 nb + b entries) | window rows (W x w) | window right-hand side (W)
@@ -91,14 +97,14 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
     double *win, *rv;
     if constexpr (SMEM) {
         win = (double *)(band_smem + (size_t)(2 * nb + b) * sizeof(int64_t));
-        rv = win + (size_t)W * w;
+        rv = win + (size_t)W * ws;
     } else {
         win = a;
         rv = rhs;
     }
     auto slot = [&](int i) -> Off { return SMEM ? (Off)(i % W) : (Off)i; };
     // entry (i, j) of a resident row, j in [i - b, i]
-    auto E = [&](int i, int j) -> double & { return win[slot(i) * (Off)w + (j - i + b)]; };
+    auto E = [&](int i, int j) -> double & { return win[slot(i) * (Off)ws + (j - i + b)]; };
     auto RV = [&](int i) -> double & { return rv[slot(i)]; };
     // rows [r0, r1) of the band (and of the right-hand side) into their window slots, asynchronously
     auto fetch = [&](int r0, int r1) {
@@ -106,10 +112,11 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
             r0 = max(r0, 0);
             r1 = min(r1, n);
             if (r1 <= r0) return;
-            int64_t cnt = (int64_t)(r1 - r0) * w;
-            for (int64_t t = tid; t < cnt; t += kThreads) {
-                int i = r0 + (int)(t / w), c = (int)(t % w);
-                cp8(win + (size_t)(i % W) * w + c, a + (size_t)i * w + c);
+            // a warp per row, a lane per entry
+            for (int i = r0 + warp; i < r1; i += kThreads / 32) {
+                double *d = win + (size_t)(i % W) * ws;
+                const double *g = a + (size_t)i * w;
+                for (int c = lane; c < w; c += 32) cp8(d + c, g + c);
             }
             if (rhs)
                 for (int i = r0 + tid; i < r1; i += kThreads) cp8(rv + (i % W), rhs + i);
@@ -119,13 +126,12 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
     // rows [r0, r1) are final: back to global memory
     auto retire = [&](int r0, int r1, bool rows) {
         if constexpr (SMEM) {
-            if (rows) {
-                int64_t cnt = (int64_t)(r1 - r0) * w;
-                for (int64_t t = tid; t < cnt; t += kThreads) {
-                    int i = r0 + (int)(t / w), c = (int)(t % w);
-                    a[(size_t)i * w + c] = win[(size_t)(i % W) * w + c];
+            if (rows)
+                for (int i = r0 + warp; i < r1; i += kThreads / 32) {
+                    const double *d = win + (size_t)(i % W) * ws;
+                    double *g = a + (size_t)i * w;
+                    for (int c = lane; c < w; c += 32) g[c] = d[c];
                 }
-            }
             if (rhs)
                 for (int i = r0 + tid; i < r1; i += kThreads) rhs[i] = rv[i % W];
         }
@@ -146,7 +152,8 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
     }
     if constexpr (SMEM) {
         int r1 = min(n, W);
-        for (int64_t t = tid; t < (int64_t)r1 * w; t += kThreads) win[t] = a[t];
+        for (int i = warp; i < r1; i += kThreads / 32)
+            for (int c = lane; c < w; c += 32) win[(size_t)i * ws + c] = a[(size_t)i * w + c];
         if (rhs)
             for (int i = tid; i < r1; i += kThreads) rv[i] = rhs[i];
     }
@@ -158,21 +165,96 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
         const int last = min(n - 1, k1 - 1 + b);  // last row the panel's columns reach
         for (int t = tid; t <= last - k0; t += kThreads) {
             int i = k0 + t;
-            rowoff[t] = slot(i) * (Off)w - i + b;
+            rowoff[t] = slot(i) * (Off)ws - i + b;
         }
-        if (tid == 0) do_pivot(k0);
+        const int np = k1 - k0, R = last - k0 + 1;  // panel columns; panel rows (relative to k0)
+        const bool blocked = SMEM && R <= 32 * kBlkRows;
+        if (!blocked && tid == 0) do_pivot(k0);
         __syncthreads();
         if (s_bad >= 0) break;
         auto P = [&](int i, int j) -> double & { return win[rowoff[i - k0] + j]; };
 
-        // A: the panel's columns. Rows r = 0 .. R - 1 of the panel (relative to k0); with the window in shared
-        // memory and at most kOwn rows per thread, every thread keeps the entries of one panel column (ct) in
-        // registers, rows rt, rt + step, ..., and a column step is: scale column kk (one row per thread, into
-        // the window and lcol), barrier, each thread subtracts column kk's products from its entries (the owners
-        // of column kk + 1 then hand it to stage[] and its pivot is taken), barrier.
-        const int np = k1 - k0, R = last - k0 + 1;
+        // A: the panel's columns, in blocks of eight when the panel has at most 32 kBlkRows rows: warp 0 factors
+        // a block in registers (lane l holds rows J + l + 32 q of its eight columns; pivots and column entries
+        // travel by shuffles), barrier, every warp subtracts the block's products from the panel's later columns
+        // (one column per lane, rows split over the warps), barrier.
         const int lg = nb == 32 ? 5 : nb == 16 ? 4 : 3, step = kThreads >> lg;
-        if (SMEM && R <= kStageRows && (R + step - 1) / step <= kOwn && (1 << lg) == nb) {
+        if (blocked) {
+            for (int J = 0; J < np; J += 8) {
+                const int nc = min(8, np - J);
+                if (warp == 0) {
+                    double v[kBlkRows][8];
+#pragma unroll
+                    for (int q = 0; q < kBlkRows; q++)
+#pragma unroll
+                        for (int cc = 0; cc < 8; cc++) {
+                            int r = J + lane + 32 * q, c = J + cc;
+                            v[q][cc] = (cc < nc && r < R && r >= c && r - c <= b) ? P(k0 + r, k0 + c) : 0.0;
+                        }
+                    bool bad = false;
+#pragma unroll
+                    for (int cc = 0; cc < 8; cc++) {
+                        if (bad || cc >= nc) continue;  // warp-uniform
+                        const int c = J + cc;
+                        const double piv = __shfl_sync(FULL, v[0][cc], cc);  // row c sits on lane cc
+                        if (!(piv > 0) || isnan(piv)) {
+                            if (lane == 0) {
+                                s_bad = k0 + c;
+                                *pivot = piv;
+                            }
+                            bad = true;
+                            continue;
+                        }
+                        const double lkk = sqrt(piv);
+                        if (lane == cc) v[0][cc] = lkk;
+#pragma unroll
+                        for (int q = 0; q < kBlkRows; q++) {
+                            int r = J + lane + 32 * q;
+                            if (r > c && r < R && r - c <= b) v[q][cc] = v[q][cc] / lkk;
+                        }
+#pragma unroll
+                        for (int c2 = 0; c2 < 8; c2++) {
+                            if (c2 <= cc || c2 >= nc) continue;
+                            const double l2 = __shfl_sync(FULL, v[0][cc], c2);  // L(J + c2, c)
+#pragma unroll
+                            for (int q = 0; q < kBlkRows; q++) {
+                                int r = J + lane + 32 * q;
+                                if (r >= J + c2 && r < R && r <= c + b) v[q][c2] = v[q][c2] - v[q][cc] * l2;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < kBlkRows; q++)
+#pragma unroll
+                        for (int cc = 0; cc < 8; cc++) {
+                            int r = J + lane + 32 * q, c = J + cc;
+                            if (cc < nc && r < R && r >= c && r - c <= b) P(k0 + r, k0 + c) = v[q][cc];
+                        }
+                }
+                __syncthreads();
+                if (s_bad >= 0) break;
+                if (J + 8 < np) {
+                    const int c = J + 8 + lane;  // one later panel column per lane, rows over the warps
+                    if (c < np) {
+                        double lc[8];
+#pragma unroll
+                        for (int cc = 0; cc < 8; cc++) lc[cc] = (cc < nc && c - (J + cc) <= b) ? P(k0 + c, k0 + J + cc) : 0.0;
+                        for (int r = c + warp; r < R && r <= c + b; r += kThreads / 32) {
+                            double e = P(k0 + r, k0 + c);
+#pragma unroll
+                            for (int cc = 0; cc < 8; cc++)
+                                if (cc < nc && r - (J + cc) <= b) e = e - P(k0 + r, k0 + J + cc) * lc[cc];
+                            P(k0 + r, k0 + c) = e;
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+        } else if (SMEM && R <= kStageRows && (R + step - 1) / step <= kOwn && (1 << lg) == nb) {
+            // every thread keeps the entries of one panel column (ct) in registers, rows rt, rt + step, ...; a
+            // column step is: scale column kk (one row per thread, into the window and lcol), barrier, each
+            // thread subtracts column kk's products from its entries (the owners of column kk + 1 then hand it
+            // to stage[] and its pivot is taken), barrier
             const int ct = tid & (nb - 1), rt = tid >> lg;
             double v[kOwn];
 #pragma unroll
@@ -256,16 +338,16 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
                     if (ti == q) continue;  // the middle tile row of an odd count is covered by the first branch
                 }
                 const int ib = k1 + 4 * ti, jb = k1 + 4 * tj;
+                // rows past the panel's reach borrow row ib's (or jb's) entries: computed, never stored
                 Off pi[4], pj[4];
                 int kf[4];
-                bool iv[4], jv[4];
+                bool iv[4];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     int i = ib + u, j = jb + u;
                     iv[u] = i <= last;
-                    jv[u] = j <= last;
-                    pi[u] = iv[u] ? rowoff[i - k0] : 0;
-                    pj[u] = jv[u] ? rowoff[j - k0] : 0;
+                    pi[u] = rowoff[(iv[u] ? i : ib) - k0];
+                    pj[u] = rowoff[(j <= last ? j : jb) - k0];
                     kf[u] = max(k0, i - b);
                 }
                 double s[4][4];
@@ -273,18 +355,44 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
                 for (int u = 0; u < 4; u++)
 #pragma unroll
                     for (int v = 0; v < 4; v++) s[u][v] = (iv[u] && jb + v <= ib + u) ? win[pi[u] + jb + v] : 0.0;
-                for (int k = kf[0]; k < k1; k++) {
+                // the first rows' earliest columns lie outside the later rows' band: those few steps are masked
+                const int kfull = min(k1, kf[3]);
+                for (int k = kf[0]; k < kfull; k++) {
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        if (k < kf[u]) continue;
+                        double li = win[pi[u] + k];
+#pragma unroll
+                        for (int v = 0; v < 4; v++)
+                            if (jb + v <= ib + u) s[u][v] = s[u][v] - li * win[pj[v] + k];
+                    }
+                }
+                // every entry of the tile takes every remaining step: loads one step ahead
+                if (kfull < k1) {
                     double li[4], lj[4];
 #pragma unroll
                     for (int u = 0; u < 4; u++) {
-                        li[u] = (iv[u] && k >= kf[u]) ? win[pi[u] + k] : 0.0;
-                        lj[u] = (jv[u] && k >= jb + u - b) ? win[pj[u] + k] : 0.0;
+                        li[u] = win[pi[u] + kfull];
+                        lj[u] = win[pj[u] + kfull];
                     }
+                    for (int k = kfull; k < k1; k++) {
+                        double ni[4], nj[4];
+                        const int kn = min(k + 1, k1 - 1);
 #pragma unroll
-                    for (int u = 0; u < 4; u++)
+                        for (int u = 0; u < 4; u++) {
+                            ni[u] = win[pi[u] + kn];
+                            nj[u] = win[pj[u] + kn];
+                        }
 #pragma unroll
-                        for (int v = 0; v < 4; v++)
-                            if (k >= kf[u]) s[u][v] = s[u][v] - li[u] * lj[v];
+                        for (int u = 0; u < 4; u++)
+#pragma unroll
+                            for (int v = 0; v < 4; v++) s[u][v] = s[u][v] - li[u] * lj[v];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            li[u] = ni[u];
+                            lj[u] = nj[u];
+                        }
+                    }
                 }
 #pragma unroll
                 for (int u = 0; u < 4; u++)
@@ -333,12 +441,20 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
         const int i0 = max(0, i1 - nb);
         const int np = i1 - i0;
         if (warp == 0) {
-            double y = lane < np ? RV(i0 + lane) : 0.0;
+            // lane l: row i0 + l; the block's row offsets go to brow[] for the update of the rows above
+            Off ro = lane < np ? slot(i0 + lane) * (Off)ws - (i0 + lane) + b : 0;
+            brow[lane] = ro;
+            double y = lane < np ? RV(i0 + lane) : 0.0, d = lane < np ? win[ro + i0 + lane] : 1.0;
+            __syncwarp();
+            double e = 0.0;  // L(i, i0 + lane) of the current step's row i, loaded one step ahead
+            if (np >= 1 && lane < np - 1 && np - 1 - lane <= b) e = win[brow[np - 1] + i0 + lane];
             for (int kk = np - 1; kk >= 0; kk--) {
-                const int i = i0 + kk;
-                if (lane == kk) y = y / E(i, i);
-                double xi = __shfl_sync(FULL, y, kk);
-                if (lane < kk && kk - lane <= b) y = y - E(i, i0 + lane) * xi;
+                double en = 0.0;
+                if (kk >= 1 && lane < kk - 1 && kk - 1 - lane <= b) en = win[brow[kk - 1] + i0 + lane];
+                if (lane == kk) y = y / d;
+                const double xi = __shfl_sync(FULL, y, kk);
+                if (lane < kk && kk - lane <= b) y = y - e * xi;
+                e = en;
             }
             if (lane < np) {
                 RV(i0 + lane) = y;
@@ -348,7 +464,7 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
         __syncthreads();
         for (int k = max(0, i0 - b) + tid; k < i0; k += kThreads) {
             double rr = RV(k);
-            for (int i = min(i1 - 1, k + b); i >= i0; i--) rr = rr - E(i, k) * xs[i - i0];
+            for (int i = min(i1 - 1, k + b); i >= i0; i--) rr = rr - win[brow[i - i0] + k] * xs[i - i0];
             RV(k) = rr;
         }
         __syncthreads();

@@ -498,10 +498,8 @@ void WarmStartNet::add_samples_device(const float *d_x, const float *d_t, int64_
             cuda_check(cudaMemcpyAsync(nt.p, dt_.p, sizeof(float) * count_ * NOUT, cudaMemcpyDeviceToDevice, s), "D2D");
         }
         cuda_check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-        std::swap(dx_.p, nx.p);
-        std::swap(dx_.n, nx.n);
-        std::swap(dt_.p, nt.p);
-        std::swap(dt_.n, nt.n);
+        swap_buf(dx_, nx);
+        swap_buf(dt_, nt);
         cap_ = cap;
     }
     cuda_check(cudaMemcpyAsync(dx_.p + count_ * NIN, d_x, sizeof(float) * n * NIN, cudaMemcpyDeviceToDevice, s), "D2D");

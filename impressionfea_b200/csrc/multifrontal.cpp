@@ -10,6 +10,7 @@
 #include <chrono>
 #include <climits>
 #include <functional>
+#include <memory>
 #include <numeric>
 #include <thread>
 
@@ -24,21 +25,37 @@ namespace {
 // separator is numbered after both halves, which recurse; leaves keep their order. A node can only neighbour the
 // other side from within reach[ax] of the plane (its longest edge along that axis), so the boundary scans cover a
 // slab of the sorted set, not all of it.
+// The two halves of a cut share no node, so from depth 1 to kParDepth - 1 one of them recurses on a new host
+// thread; every subtree writes its own fragment of the reverse order and the fragments are joined in the
+// sequential order, so the result does not depend on the threads. Set stamps come from one atomic counter, so
+// that no two sets (of any thread) share a stamp.
+// A set mark read by one thread while another writes it (a neighbour in the other half): relaxed atomic access.
+struct SetMark {
+    std::atomic<int32_t> v{0};
+    operator int32_t() const { return v.load(std::memory_order_relaxed); }
+    SetMark &operator=(int32_t x)
+    {
+        v.store(x, std::memory_order_relaxed);
+        return *this;
+    }
+};
+
 struct CoordNd {
-    static constexpr int kLeaf = 32, kCoverDepth = 2;
+    static constexpr int kLeaf = 32, kCoverDepth = 2, kParDepth = 4;
     int nb;
     const int *gp, *gi;
     const double *x;
-    std::vector<int32_t> mark, perm_rev, loc, vis;  // perm_rev: nodes in reverse elimination order
+    std::unique_ptr<SetMark[]> mark;
+    std::vector<int32_t> loc, vis;
     std::vector<double> reach[3];
-    int stamp = 0;
+    std::atomic<int> stamp{0};
 
     double X(int v, int ax) const { return x[3 * (size_t)v + ax]; }
     bool less(int a, int b, int ax) const { return X(a, ax) < X(b, ax) || (X(a, ax) == X(b, ax) && a < b); }
 
     void run(int32_t *pnode)
     {
-        mark.assign(nb, 0);
+        mark.reset(new SetMark[nb]);
         loc.assign(nb, -1);
         for (int ax = 0; ax < 3; ax++) {
             reach[ax].assign(nb, 0.0);
@@ -47,8 +64,9 @@ struct CoordNd {
         }
         std::vector<int> all(nb);
         std::iota(all.begin(), all.end(), 0);
-        perm_rev.clear();
-        split(all, 0);
+        std::vector<int32_t> perm_rev;  // nodes in reverse elimination order
+        perm_rev.reserve(nb);
+        split(all, 0, perm_rev);
         for (int k = 0; k < nb; k++) pnode[k] = perm_rev[nb - 1 - k];
     }
 
@@ -171,7 +189,7 @@ struct CoordNd {
         return C;
     }
 
-    void split(std::vector<int> &set, int depth)
+    void split(std::vector<int> &set, int depth, std::vector<int32_t> &perm_rev)
     {
         int n = (int)set.size();
         if (n <= kLeaf) {
@@ -233,8 +251,17 @@ struct CoordNd {
         for (int i = (int)S.size() - 1; i >= 0; i--) perm_rev.push_back(S[i]);
         for (auto &v : arr) std::vector<int>().swap(v);
         std::vector<int>().swap(set);
-        split(R, depth + 1);
-        split(L, depth + 1);
+        if (depth >= 1 && depth < kParDepth && (int)(L.size() + R.size()) > 4096) {
+            std::vector<int32_t> pr, pl;
+            std::thread t([&] { split(R, depth + 1, pr); });
+            split(L, depth + 1, pl);
+            t.join();
+            perm_rev.insert(perm_rev.end(), pr.begin(), pr.end());
+            perm_rev.insert(perm_rev.end(), pl.begin(), pl.end());
+        } else {
+            split(R, depth + 1, perm_rev);
+            split(L, depth + 1, perm_rev);
+        }
     }
 };
 }  // namespace
@@ -437,44 +464,84 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
         int last = c0[s] + ncol[s] - 1;
         if (parent_c[last] >= 0) parent[s] = sn_of[parent_c[last]];
     }
-    // 6. row structures (children precede parents in postorder)
+    // 6. row structures (children precede parents in postorder). The subtrees hanging at depth kRowDepth below the
+    //    roots are disjoint postorder ranges and are built on host threads; the supernodes above them follow in
+    //    order. Each supernode's structure is its own and its children's rows, so the result does not depend on the
+    //    split.
     std::vector<std::vector<int32_t>> strc(nsuper);
     std::vector<std::vector<int32_t>> kids(nsuper);
     for (int s = 0; s < nsuper; s++)
         if (parent[s] >= 0) kids[parent[s]].push_back(s);
     {
-        std::vector<int32_t> mark(ns, -1);
-        std::vector<uint64_t> bits((size_t)ns / 64 + 1, 0);  // ascending order of a row set through a bitmap
-        for (int s = 0; s < nsuper; s++) {
-            int first = c0[s], end = c0[s] + ncol[s];
-            auto &v = strc[s];
-            int lo = ns, hi = -1;
-            auto add = [&](int i) {
-                if (i >= end && mark[i] != s) {
-                    mark[i] = s;
-                    v.push_back(i);
-                    lo = std::min(lo, i);
-                    hi = std::max(hi, i);
+        std::atomic<bool> bad_counts{false};
+        auto build_range = [&](const std::vector<int32_t> &order, std::vector<int32_t> &mark, std::vector<uint64_t> &bits) {
+            for (int s : order) {
+                int first = c0[s], end = c0[s] + ncol[s];
+                auto &v = strc[s];
+                int lo = ns, hi = -1;
+                auto add = [&](int i) {
+                    if (i >= end && mark[i] != s) {
+                        mark[i] = s;
+                        v.push_back(i);
+                        lo = std::min(lo, i);
+                        hi = std::max(hi, i);
+                    }
+                };
+                for (int j = first; j < end; j++) {
+                    int d = perm[j];
+                    for (int32_t p = scp[d]; p < scp[d + 1]; p++) add(pinv[sri[p]]);
                 }
-            };
-            for (int j = first; j < end; j++) {
-                int d = perm[j];
-                for (int32_t p = scp[d]; p < scp[d + 1]; p++) add(pinv[sri[p]]);
-            }
-            for (int c : kids[s])
-                for (int i : strc[c]) add(i);
-            if (v.size() < 64 || (size_t)(hi - lo) > 64 * v.size()) {
-                std::sort(v.begin(), v.end());
-            } else {
-                for (int i : v) bits[(size_t)(i - lo) >> 6] |= 1ull << ((i - lo) & 63);
-                size_t k = 0, nw = (size_t)(hi - lo) / 64 + 1;
-                for (size_t w = 0; w < nw; w++) {
-                    for (uint64_t b = bits[w]; b; b &= b - 1) v[k++] = lo + (int)(64 * w) + __builtin_ctzll(b);
-                    bits[w] = 0;
+                for (int c : kids[s])
+                    for (int i : strc[c]) add(i);
+                if (v.size() < 64 || (size_t)(hi - lo) > 64 * v.size()) {
+                    std::sort(v.begin(), v.end());
+                } else {
+                    for (int i : v) bits[(size_t)(i - lo) >> 6] |= 1ull << ((i - lo) & 63);
+                    size_t k = 0, nw = (size_t)(hi - lo) / 64 + 1;
+                    for (size_t w = 0; w < nw; w++) {
+                        for (uint64_t b = bits[w]; b; b &= b - 1) v[k++] = lo + (int)(64 * w) + __builtin_ctzll(b);
+                        bits[w] = 0;
+                    }
                 }
+                if ((int64_t)v.size() + ncol[s] != cc[first]) bad_counts = true;
             }
-            if ((int64_t)v.size() + ncol[s] != cc[first]) return "internal error: supernode structure does not match the column counts";
+        };
+        // depth below the roots; the subtree of s is the postorder range [first_sn[s], s]
+        constexpr int kRowDepth = 3;
+        std::vector<int32_t> depth(nsuper, 0), first_sn(nsuper);
+        for (int s = nsuper - 1; s >= 0; s--) depth[s] = parent[s] >= 0 ? depth[parent[s]] + 1 : 0;
+        for (int s = 0; s < nsuper; s++) first_sn[s] = s;
+        for (int s = 0; s < nsuper; s++)
+            if (parent[s] >= 0) first_sn[parent[s]] = std::min(first_sn[parent[s]], first_sn[s]);
+        std::vector<std::vector<int32_t>> ranges;
+        std::vector<uint8_t> in_range(nsuper, 0);
+        if (nsuper >= 256)
+            for (int s = 0; s < nsuper; s++)
+                if (depth[s] == kRowDepth) {
+                    ranges.emplace_back();
+                    for (int q = first_sn[s]; q <= s; q++) ranges.back().push_back(q), in_range[q] = 1;
+                }
+        std::vector<int32_t> top;
+        for (int s = 0; s < nsuper; s++)
+            if (!in_range[s]) top.push_back(s);
+        if (!ranges.empty()) {
+            std::vector<std::thread> th;
+            std::atomic<int> next{0};
+            int nth = (int)std::min<size_t>(ranges.size(), std::max(1u, std::thread::hardware_concurrency()));
+            for (int t = 0; t < nth; t++)
+                th.emplace_back([&] {
+                    std::vector<int32_t> mark(ns, -1);
+                    std::vector<uint64_t> bits((size_t)ns / 64 + 1, 0);
+                    for (int r; (r = next.fetch_add(1)) < (int)ranges.size();) build_range(ranges[r], mark, bits);
+                });
+            for (auto &t : th) t.join();
         }
+        {
+            std::vector<int32_t> mark(ns, -1);
+            std::vector<uint64_t> bits((size_t)ns / 64 + 1, 0);
+            build_range(top, mark, bits);
+        }
+        if (bad_counts) return "internal error: supernode structure does not match the column counts";
     }
     if (B > 1) {  // node numbering -> equation numbering
         std::vector<int32_t> pn(perm);
@@ -483,14 +550,23 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
         for (int k = 0; k < ns; k++)
             for (int c = 0; c < B; c++) perm[k * B + c] = pn[k] * B + c;
         for (int k = 0; k < n; k++) pinv[perm[k]] = k;
-        for (int s = 0; s < nsuper; s++) {
+        auto expand = [&](int s) {
             c0[s] *= B;
             ncol[s] *= B;
             std::vector<int32_t> v(strc[s].size() * B);
             for (size_t k = 0; k < strc[s].size(); k++)
                 for (int c = 0; c < B; c++) v[k * B + c] = strc[s][k] * B + c;
             strc[s] = std::move(v);
-        }
+        };
+        int nth = nsuper < 256 ? 1 : (int)std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+        std::atomic<int> next{0};
+        auto worker = [&] {
+            for (int s; (s = next.fetch_add(1)) < nsuper;) expand(s);
+        };
+        std::vector<std::thread> th;
+        for (int t = 1; t < nth; t++) th.emplace_back(worker);
+        worker();
+        for (auto &t : th) t.join();
     }
     // 6b. relaxed amalgamation: merge a supernode into its parent when it is the parent's contiguous (last) child
     //     and the explicit zeros this adds stay small; chains inside a separator collapse into one front.

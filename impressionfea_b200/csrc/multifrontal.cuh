@@ -541,96 +541,85 @@ __device__ __forceinline__ void dev_wide_acc(Dev<T> D, int s, const T *y, int ch
     }
 }
 
-// The row-oriented GEMVs below give each CTA 16 rows and let its 16 warps split the columns: a half-warp reads
-// 16 consecutive rows of one column (128 contiguous bytes), the 32 half-warps of the CTA take columns
-// sub, sub + 32, ... so every thread keeps several independent loads in flight. Row tiles are visited bottom-up
-// (the longest rows of a triangular operand first).
-constexpr int RT = 16;
-
-// y1 = X acc1 (X lower triangular), row tile `tile` (counted from the bottom) of front s.
-template <typename T>
-__device__ __forceinline__ void dev_wide_fwd_y(Dev<T> D, int s, int tile, T *y, T *Y1)
+// The forward GEMVs with the row tile sized to the level: a CTA takes 32 RG rows (warp w: the 32 consecutive
+// rows of row group w % RG, i.e. 128 contiguous bytes of each FP32 column, and the columns w / RG, w / RG + CG,
+// ..., CG = 16 / RG), sixteen loads in flight per thread; the column groups' partial sums meet in shared memory
+// and are added in group order. RG grows as the level's pivot blocks narrow, so that a thread still has some
+// tens of loads to issue.
+template <typename T, int RG>
+__device__ __forceinline__ T rows_dot(const T *__restrict__ A, int64_t ld, int row, int nrows, int c_end,
+                                      const T *__restrict__ v, bool lower)
 {
-    __shared__ T part[32][RT + 1];
-    int nc = D.ncol[s], c0 = D.c0[s], ntile = (nc + RT - 1) / RT;
-    if (tile >= ntile) return;
-    int r0 = (ntile - 1 - tile) * RT;
-    const T *X = D.Xinv + D.xinv_off[s];
-    const T *acc = D.Abig + D.idx_start[s];
-    int lane = threadIdx.x & 31, sub = (lane >> 4) + 2 * (threadIdx.x >> 5), rr = lane & (RT - 1);
-    int r = r0 + rr, cend = min(nc, r0 + RT);
-    T v = 0;
-    if (r < nc) {
-#pragma unroll 8
-        for (int c = sub; c < cend; c += 32)
-            if (c <= r) v = fma(X[(int64_t)c * nc + r], acc[c], v);
+    constexpr int CG = 16 / RG;
+    const int cg = (threadIdx.x >> 5) / RG;
+    T acc = 0;
+    if (row < nrows) {
+        const int ce = lower ? min(c_end, row + 1) : c_end;
+#pragma unroll 16
+        for (int c = cg; c < ce; c += CG) acc = fma(A[(int64_t)c * ld + row], __ldg(v + c), acc);
     }
-    part[sub][rr] = v;
+    return acc;
+}
+
+// y1 = X acc1 (X lower triangular), 32 RG rows per CTA, row tiles counted from the bottom (longest rows first)
+template <typename T, int RG>
+static __global__ void __launch_bounds__(512) k_wide_fwd_y2(Dev<T> D, const int32_t *__restrict__ fronts, T *y, T *Y1)
+{
+    constexpr int RTT = 32 * RG, CG = 16 / RG;
+    __shared__ T part[CG][RTT];
+    const int s = fronts[blockIdx.y];
+    const int nc = D.ncol[s], c0 = D.c0[s], ntile = (nc + RTT - 1) / RTT;
+    if ((int)blockIdx.x >= ntile) return;
+    const int r0 = (ntile - 1 - blockIdx.x) * RTT, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rr = 32 * (warp % RG) + lane;
+    T v = rows_dot<T, RG>(D.Xinv + D.xinv_off[s], nc, r0 + rr, nc, min(nc, r0 + RTT), D.Abig + D.idx_start[s], true);
+    part[warp / RG][rr] = v;
     __syncthreads();
-    if (threadIdx.x < RT && r0 + (int)threadIdx.x < nc) {
+    if ((int)threadIdx.x < RTT && r0 + (int)threadIdx.x < nc) {
         T t = 0;
-        for (int q = 0; q < 32; q++) t += part[q][threadIdx.x];
+#pragma unroll
+        for (int q = 0; q < CG; q++) t += part[q][threadIdx.x];
         y[c0 + r0 + threadIdx.x] = t;
         Y1[D.idx_start[s] + r0 + threadIdx.x] = t;
     }
 }
-template <typename T>
-static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32_t *__restrict__ fronts, T *y, T *Y1)
-{
-    dev_wide_fwd_y(D, fronts[blockIdx.y], blockIdx.x, y, Y1);
-}
 
-// update vector t = -acc2 + L21 y1, row tile `tile` of front s.
-template <typename T>
-__device__ __forceinline__ void dev_wide_fwd_t(Dev<T> D, int s, int tile, const T *Y1)
+// update vector t = -acc2 + L21 y1, 32 RG rows per CTA
+template <typename T, int RG>
+static __global__ void __launch_bounds__(512) k_wide_fwd_t2(Dev<T> D, const int32_t *__restrict__ fronts, const T *Y1)
 {
-    __shared__ T part[32][RT + 1];
-    int ms = D.m[s], nc = D.ncol[s], nr = ms - nc;
-    int i0 = tile * RT;
+    constexpr int RTT = 32 * RG, CG = 16 / RG;
+    __shared__ T part[CG][RTT];
+    const int s = fronts[blockIdx.y];
+    const int ms = D.m[s], nc = D.ncol[s], nr = ms - nc, i0 = blockIdx.x * RTT;
     if (i0 >= nr) return;
-    const T *F = D.F + D.front_off[s] + nc;
-    const T *y1 = Y1 + D.idx_start[s];
-    int lane = threadIdx.x & 31, sub = (lane >> 4) + 2 * (threadIdx.x >> 5), rr = lane & (RT - 1);
-    int i = i0 + rr;
-    T v = 0;
-    if (i < nr) {
-#pragma unroll 8
-        for (int k = sub; k < nc; k += 32) v = fma(F[(int64_t)k * ms + i], y1[k], v);
-    }
-    part[sub][rr] = v;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, rr = 32 * (warp % RG) + lane;
+    T v = rows_dot<T, RG>(D.F + D.front_off[s] + nc, ms, i0 + rr, nr, nc, Y1 + D.idx_start[s], false);
+    part[warp / RG][rr] = v;
     __syncthreads();
-    if (threadIdx.x < RT && i0 + (int)threadIdx.x < nr) {
+    if ((int)threadIdx.x < RTT && i0 + (int)threadIdx.x < nr) {
         T t = 0;
-        for (int q = 0; q < 32; q++) t += part[q][threadIdx.x];
+#pragma unroll
+        for (int q = 0; q < CG; q++) t += part[q][threadIdx.x];
         int ii = i0 + threadIdx.x;
         D.U[D.uvec_start[s] + ii] = -D.Abig[D.idx_start[s] + nc + ii] + t;
     }
 }
-template <typename T>
-static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32_t *__restrict__ fronts, const T *Y1)
-{
-    dev_wide_fwd_t(D, fronts[blockIdx.y], blockIdx.x, Y1);
-}
 
-// z = y1 - L21^T x2, one warp per pivot column; x2 is gathered into shared memory once per CTA.
+// z = y1 - L21^T x2, one warp per pivot column; x2 is read through the front's row indices as the column
+// streams (the CTA's warps read the same entries, from L1), sixteen column loads in flight per lane.
 template <typename T>
 __device__ __forceinline__ void dev_wide_bwd_z(Dev<T> D, int s, int tile, const T *x, T *Z)
 {
-    extern __shared__ __align__(16) unsigned char xs_raw[];
-    T *xs = (T *)xs_raw;
     int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s], nr = ms - nc;
-    int kbase = tile * (blockDim.x >> 5);
-    if (kbase >= nc) return;
-    const int32_t *ix = D.idx + D.idx_start[s] + nc;
-    for (int i = threadIdx.x; i < nr; i += blockDim.x) xs[i] = x[ix[i]];
-    __syncthreads();
-    int k = kbase + (threadIdx.x >> 5);
+    int k = tile * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (k >= nc) return;
-    const T *col = D.F + D.front_off[s] + (int64_t)k * ms + nc;
+    const int32_t *__restrict__ ix = D.idx + D.idx_start[s] + nc;
+    const T *__restrict__ col = D.F + D.front_off[s] + (int64_t)k * ms + nc;
     int lane = threadIdx.x & 31;
     T v = 0;
-#pragma unroll 8
-    for (int i = lane; i < nr; i += 32) v = fma(col[i], xs[i], v);
+#pragma unroll 16
+    for (int i = lane; i < nr; i += 32) v = fma(col[i], __ldg(x + __ldg(ix + i)), v);
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) Z[D.idx_start[s] + k] = x[c0 + k] - v;
 }
@@ -874,16 +863,39 @@ static __global__ void __launch_bounds__(256) k_pack_sp(Dev<float> D, const int3
 }
 
 // The trailing update of a super-panel on the tensor cores: the region of rows and columns from kend on of every
-// listed front, C -= A A^T with A its packed pivot columns [K0, kend). Persistent CTAs (one per SM) walk the
-// region's 128 x 128 lower tiles; per tile, K comes in stages of 32 columns through a ring of three shared-memory
-// slots. Warp 0 (one lane) copies a stage's four operand parts into a free slot with bulk copies; warp 1 (one
-// lane) issues its twelve MMAs (4 K steps x 3 split terms) into one of two tensor-memory accumulators and
-// releases the slot when they complete; warps 4..11 read a finished accumulator (warp w: lanes 32 (w % 4) .., one
-// half of the columns), subtract it from the tile's old values in the front and hand the accumulator back, while
-// the MMAs of the next tile run into the other one. Every wait is bounded: one that gives up sets *err and the
-// CTA stops issuing work, waits for what it issued and releases its tensor memory.
+// listed front, C -= A A^T with A its packed pivot columns [K0, kend). Persistent CTAs (one per SM) walk the 128 x
+// 128 lower tiles of all listed fronts as one sequence (front f owns tiles tstart[f] .. tstart[f + 1] - 1), so that
+// fronts of different sizes share the SMs evenly; per tile, K comes in stages of 32 columns through a ring of
+// three shared-memory slots. Warp 0 (one lane) copies a stage's four operand parts into a free slot with bulk
+// copies; warp 1 (one lane) issues its twelve MMAs (4 K steps x 3 split terms) into one of two tensor-memory
+// accumulators and releases the slot when they complete; warps 4..11 read a finished accumulator (warp w: lanes
+// 32 (w % 4) .., one half of the columns), subtract it from the tile's old values in the front and hand the
+// accumulator back, while the MMAs of the next tile run into the other one. Every wait is bounded: one that gives
+// up sets *err and the CTA stops issuing work, waits for what it issued and releases its tensor memory.
+struct SpTile {
+    int s, ms, kend, nst, ti, tj;
+    const unsigned char *pb;
+    float *F;
+};
+__device__ __forceinline__ SpTile sp_tile(const Dev<float> &D, const int32_t *__restrict__ fronts,
+                                          const int32_t *__restrict__ tstart, int K0, const int64_t *__restrict__ pk_off,
+                                          const float4 *P, int g, int &f)
+{
+    while (tstart[f + 1] <= g) f++;  // g only grows along a CTA's sequence
+    SpTile t;
+    t.s = fronts[f];
+    t.ms = D.m[t.s];
+    t.kend = min(K0 + tcu::SPW, D.ncol[t.s]);
+    t.nst = (t.kend - K0 + tcu::KS - 1) / tcu::KS;
+    tcu::tri_tile(g - tstart[f], t.ti, t.tj);
+    t.pb = (const unsigned char *)P + pk_off[t.s];
+    t.F = D.F + D.front_off[t.s];
+    return t;
+}
+
 static __global__ void __launch_bounds__(tcu::kThreads, 1) k_update_sp(Dev<float> D, const int32_t *__restrict__ fronts,
-                                                                      int K0, const int64_t *__restrict__ pk_off,
+                                                                      const int32_t *__restrict__ tstart, int nf, int K0,
+                                                                      const int64_t *__restrict__ pk_off,
                                                                       const float4 *__restrict__ P, int *err)
 {
     using namespace tcu;
@@ -891,14 +903,8 @@ static __global__ void __launch_bounds__(tcu::kThreads, 1) k_update_sp(Dev<float
     uint64_t *bars = (uint64_t *)(tsm + NST * kStage);  // full[NST], empty[NST], tfull[2], tempty[2], drain
     uint32_t *tslot = (uint32_t *)(bars + 2 * NST + 5);
     volatile int *abort_flag = (volatile int *)(tslot + 1);
-    const int s = fronts[blockIdx.y];
-    const int ms = D.m[s], kend = min(K0 + SPW, D.ncol[s]), K = kend - K0, nt = ms - kend;
-    if (K <= 0 || nt <= 0) return;
-    const int nti = (nt + TM - 1) / TM, ntiles = nti * (nti + 1) / 2;
-    if ((int)blockIdx.x >= ntiles) return;  // both exits come before the tensor memory is taken
-    const int nst = (K + KS - 1) / KS;
-    const unsigned char *pb = (const unsigned char *)P + pk_off[s];
-    float *F = D.F + D.front_off[s];
+    const int ntiles = tstart[nf];
+    if ((int)blockIdx.x >= ntiles) return;  // before the tensor memory is taken
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t full0 = smem_u32(bars), empty0 = full0 + 8 * NST, tfull0 = empty0 + 8 * NST, tempty0 = tfull0 + 16,
                    drain = tempty0 + 16;
@@ -929,12 +935,11 @@ static __global__ void __launch_bounds__(tcu::kThreads, 1) k_update_sp(Dev<float
 
     if (warp == 0) {
         if (lane == 0) {  // producer
-            int g = 0;
+            int g = 0, f = 0;
             for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
-                int ti, tj;
-                tri_tile(t, ti, tj);
-                const unsigned char *a = pb + ti * kRowBlock, *b = pb + tj * kRowBlock;
-                for (int st = 0; st < nst; st++, g++) {
+                const SpTile T = sp_tile(D, fronts, tstart, K0, pk_off, P, t, f);
+                const unsigned char *a = T.pb + T.ti * kRowBlock, *b = T.pb + T.tj * kRowBlock;
+                for (int st = 0; st < T.nst; st++, g++) {
                     int slot = g % NST;
                     if (!mbar_wait(empty0 + 8 * slot, ((g / NST) & 1) ^ 1)) {
                         give_up();
@@ -957,9 +962,10 @@ static __global__ void __launch_bounds__(tcu::kThreads, 1) k_update_sp(Dev<float
         }
     } else if (warp == 1) {
         if (lane == 0) {  // MMA issuer
-            int g = 0, lt = 0;
+            int g = 0, lt = 0, f = 0;
             bool issued = false;
             for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, lt++) {
+                const int nst = sp_tile(D, fronts, tstart, K0, pk_off, P, t, f).nst;
                 int acc = lt & 1;
                 if (!mbar_wait(tempty0 + 8 * acc, ((lt >> 1) & 1) ^ 1)) {
                     give_up();
@@ -997,12 +1003,13 @@ static __global__ void __launch_bounds__(tcu::kThreads, 1) k_update_sp(Dev<float
         }
     } else if (warp >= 4) {  // epilogue
         const int q = warp & 3, h = (warp - 4) >> 2;
-        int lt = 0;
+        int lt = 0, f = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
-            int ti, tj;
-            tri_tile(t, ti, tj);
+            const SpTile T = sp_tile(D, fronts, tstart, K0, pk_off, P, t, f);
+            const int ms = T.ms;
+            float *F = T.F;
             int acc = lt & 1;
-            const int gi = kend + ti * TM + 32 * q + lane, cj0 = kend + tj * TN + 64 * h;
+            const int gi = T.kend + T.ti * TM + 32 * q + lane, cj0 = T.kend + T.tj * TN + 64 * h;
             bool ok = mbar_wait(tfull0 + 8 * acc, (lt >> 1) & 1);
             if (!__all_sync(0xffffffffu, ok)) {
                 if (lane == 0) give_up();
@@ -1230,7 +1237,8 @@ template <typename T>
 class MfSolverT final : public LinearSolver {
 public:
     struct SpStep {  // one super-panel's trailing update within a level
-        int tc_off = 0, tc_cnt = 0, tc_grid = 0, tc_rb = 0;  // tensor-core fronts: list, CTAs per front, row blocks
+        int tc_off = 0, tc_cnt = 0, tc_grid = 0, tc_rb = 0;  // tensor-core fronts: list, CTAs, most row blocks
+        int tc_toff = 0;                                     // their tile-sequence prefix (tc_cnt + 1 entries)
         int si_off = 0, si_cnt = 0, si_tiles = 0;            // the other fronts: list, most 64 x 64 tiles of one
     };
     explicit MfSolverT(cudaStream_t s) : st_(s)
@@ -1491,7 +1499,7 @@ public:
         ensure_dynamic_smem((const void *)mf::k_xinv_gemm<T, 0>, (int)kPairSmem);
         ensure_dynamic_smem((const void *)mf::k_xinv_gemm<T, 1>, (int)kPairSmem);
         if (small_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the solve kernels' shared-memory window");
-        level_smem_ = std::max(small_smem_, wide_smem_);
+        level_smem_ = small_smem_;  // the wide fronts' z pass stages nothing
         ensure_dynamic_smem((const void *)mf::k_fwd_level<T>, (int)small_smem_);
         ensure_dynamic_smem((const void *)mf::k_bwd_level<T>, (int)level_smem_);
         cuda_check(cudaStreamSynchronize(st_), "cudaStreamSynchronize");
@@ -1637,8 +1645,8 @@ public:
         if constexpr (std::is_same<T, float>::value) {
             const int32_t *fl = d_sp_.p + ps.tc_off;
             mf::k_pack_sp<<<dim3(ps.tc_rb, ps.tc_cnt), 256, 0, st>>>(dev_, fl, K0, d_pk_off_.p, d_pack_.p);
-            mf::k_update_sp<<<dim3(ps.tc_grid, ps.tc_cnt), mf::tcu::kThreads, mf::tcu::kSmem, st>>>(
-                dev_, fl, K0, d_pk_off_.p, d_pack_.p, d_err_.p + 2);
+            mf::k_update_sp<<<ps.tc_grid, mf::tcu::kThreads, mf::tcu::kSmem, st>>>(
+                dev_, fl, d_sp_.p + ps.tc_toff, ps.tc_cnt, K0, d_pk_off_.p, d_pack_.p, d_err_.p + 2);
             tc_launches_++;
         }
     }
@@ -1680,7 +1688,19 @@ public:
                     }
                 }
                 ps.tc_cnt = (int)lists.size() - ps.tc_off;
-                if (ps.tc_cnt > 0) ps.tc_grid = std::min(tiles_max, std::max(1, 148 / ps.tc_cnt));
+                if (ps.tc_cnt > 0) {
+                    // the tensor-core fronts' tiles as one sequence: its prefix follows the front list
+                    ps.tc_toff = (int)lists.size();
+                    int total = 0;
+                    lists.push_back(0);
+                    for (int i = 0; i < ps.tc_cnt; i++) {
+                        int sn = lists[ps.tc_off + i], region = S.m[sn] - std::min(K0 + SPW, S.ncol[sn]);
+                        int nrb = (region + mf::tcu::TM - 1) / mf::tcu::TM;
+                        total += nrb * (nrb + 1) / 2;
+                        lists.push_back(total);
+                    }
+                    ps.tc_grid = std::min(total, 148);
+                }
                 ps.si_off = (int)lists.size();
                 for (int q = q0; q < q1 && S.ncol[lvl_sorted_[q]] > K0; q++) {
                     int sn = lvl_sorted_[q], region = S.m[sn] - std::min(K0 + SPW, S.ncol[sn]);
@@ -1767,8 +1787,16 @@ public:
                     mnc = std::max(mnc, S.ncol[big_list_[q]]);
                     mnr = std::max(mnr, S.m[big_list_[q]] - S.ncol[big_list_[q]]);
                 }
-                mf::k_wide_fwd_y<T><<<dim3((mnc + mf::RT - 1) / mf::RT, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
-                mf::k_wide_fwd_t<T><<<dim3((mnr + mf::RT - 1) / mf::RT, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
+                // rows per CTA from the level's widest pivot block: 256 rows up to 200 columns ... 32 from 800 on
+                int rg = mnc <= 200 ? 8 : mnc <= 400 ? 4 : mnc <= 800 ? 2 : 1, rt = 32 * rg;
+                dim3 gy((mnc + rt - 1) / rt, bc), gt((mnr + rt - 1) / rt, bc);
+                const int32_t *bl = d_big_.p + b0;
+                switch (rg) {
+                case 8: mf::k_wide_fwd_y2<T, 8><<<gy, 512, 0, st>>>(dev_, bl, d_y_, d_y1_); mf::k_wide_fwd_t2<T, 8><<<gt, 512, 0, st>>>(dev_, bl, d_y1_); break;
+                case 4: mf::k_wide_fwd_y2<T, 4><<<gy, 512, 0, st>>>(dev_, bl, d_y_, d_y1_); mf::k_wide_fwd_t2<T, 4><<<gt, 512, 0, st>>>(dev_, bl, d_y1_); break;
+                case 2: mf::k_wide_fwd_y2<T, 2><<<gy, 512, 0, st>>>(dev_, bl, d_y_, d_y1_); mf::k_wide_fwd_t2<T, 2><<<gt, 512, 0, st>>>(dev_, bl, d_y1_); break;
+                default: mf::k_wide_fwd_y2<T, 1><<<gy, 512, 0, st>>>(dev_, bl, d_y_, d_y1_); mf::k_wide_fwd_t2<T, 1><<<gt, 512, 0, st>>>(dev_, bl, d_y1_); break;
+                }
             }
         }
         for (int l = S.nlevels - 1; l >= 0; l--) {

@@ -942,6 +942,7 @@ bool remesh_workpiece(const RemeshInput &in, RemeshOutput &out)
         out.why = "Tetrahedral mesh is not manifold (face shared by more than two tets)";
         return false;
     }
+    if (in.on_topology) in.on_topology(x, t, M.onx, M.ony);
     std::vector<d3> stuffed = x;
     std::vector<uint8_t> contact(nn, IFEA_FREE);
     std::vector<d3> nrm = surface_normals(M, x);

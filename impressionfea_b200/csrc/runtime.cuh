@@ -8,6 +8,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/ifea_gpu.h"
@@ -46,11 +47,13 @@ inline void ensure_dynamic_smem(const void *kernel, size_t bytes)
     cur = bytes;
 }
 
-// Owning device buffer (cudaMalloc / cudaFree; contents undefined after resize).
+// Owning device buffer (cudaMalloc / cudaFree; contents undefined after resize). n is the logical length; a
+// resize within the allocation keeps it (a remeshed workpiece changes every mesh-sized buffer by a few per cent),
+// a larger one reallocates with an eighth of headroom.
 template <typename T>
 struct DBuf {
     T *p = nullptr;
-    size_t n = 0;
+    size_t n = 0, cap = 0;
     DBuf() = default;
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
@@ -59,13 +62,20 @@ struct DBuf {
     {
         if (p) cudaFree(p);
         p = nullptr;
-        n = 0;
+        n = cap = 0;
     }
     void resize(size_t count)
     {
-        if (count == n && p) return;
+        if (p && count <= cap) {
+            n = count;
+            return;
+        }
         release();
-        if (count) cuda_check(cudaMalloc((void **)&p, count * sizeof(T)), "cudaMalloc");
+        if (count) {
+            size_t c = count + count / 8;
+            cuda_check(cudaMalloc((void **)&p, c * sizeof(T)), "cudaMalloc");
+            cap = c;
+        }
         n = count;
     }
     void upload(const T *src, size_t count, cudaStream_t s)
@@ -84,6 +94,15 @@ struct DBuf {
     }
     operator T *() const { return p; }
 };
+
+// Exchange two buffers' allocations (pointer, length and capacity).
+template <typename T>
+inline void swap_buf(DBuf<T> &a, DBuf<T> &b)
+{
+    std::swap(a.p, b.p);
+    std::swap(a.n, b.n);
+    std::swap(a.cap, b.cap);
+}
 
 // Pinned host staging for scalars read back every iteration.
 template <typename T>

@@ -1011,8 +1011,8 @@ struct Forging2D {
             why = fmt2("element %d folded", e4[1]);
             return false;
         }
-        std::swap(d_x.p, d_xT.p);
-        std::swap(d_contact.p, d_cT.p);
+        swap_buf(d_x, d_xT);
+        swap_buf(d_contact, d_cT);
         gap = gapT;
         time += dt;
         return true;
@@ -1075,8 +1075,8 @@ struct Forging2D {
         if (c4[0] > 0) {
             remesh_requests++;
             if (min_quality(d_x) <= 0.05) {
-                std::swap(d_x.p, d_xT.p);
-                std::swap(d_contact.p, d_cT.p);
+                swap_buf(d_x, d_xT);
+                swap_buf(d_contact, d_cT);
             } else {
                 captured += c4[0];
             }

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <future>
 #include <thread>
 #include <vector>
 
@@ -270,6 +271,15 @@ struct Forging3D {
     std::thread sym_job;
     std::unique_ptr<MfSymbolic> sym_pre;
     std::string sym_err;
+    // a remesh starts the job as soon as the new connectivity is known: it builds that mesh's topology first
+    // (handed to set_mesh through topo_ready) and then analyses its pattern
+    std::unique_ptr<TetTopology> topo_ahead;
+    std::vector<double> ahead_x;
+    std::vector<int32_t> ahead_t;
+    std::vector<uint8_t> ahead_onx, ahead_ony;
+    std::promise<std::string> topo_promise;
+    std::future<std::string> topo_ready;
+    bool ahead_pending = false;
     double t_sym_wait = 0;
     int ordering = 1;
     std::vector<double> node_xyz;  // node coordinates when the mesh was set
@@ -442,8 +452,16 @@ struct Forging3D {
         if (sym_job.joinable()) sym_job.join();
     }
 
-    // one analysis on the calling (job) thread: coordinate order when xyz is given, else METIS
-    void analysis_job(int dev, const double *xyz, std::unique_ptr<MfSymbolic> *out, std::string *err)
+    // one analysis of tp's pattern on the calling (job) thread: coordinate order when xyz is given, else METIS
+    void analysis_job(int dev, const TetTopology *tp, const double *xyz, std::unique_ptr<MfSymbolic> *out,
+                      std::string *err)
+    {
+        const int ndof = tp->ndof;
+        const int32_t *cp = tp->col_ptr.data(), *ri = tp->row_idx.data();
+        analysis_job(dev, ndof, cp, ri, xyz, out, err);
+    }
+    void analysis_job(int dev, int ndof, const int32_t *cp, const int32_t *ri, const double *xyz,
+                      std::unique_ptr<MfSymbolic> *out, std::string *err)
     {
         cusolverSpHandle_t hsp = nullptr;
         cusparseMatDescr_t descr = nullptr;
@@ -459,7 +477,7 @@ struct Forging3D {
                 cusparseSetMatType(descr, CUSPARSE_MATRIX_TYPE_GENERAL);
                 cusparseSetMatIndexBase(descr, CUSPARSE_INDEX_BASE_ZERO);
                 std::unique_ptr<MfSymbolic> S(new MfSymbolic);
-                std::string e = S->analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), 3, hsp, descr, xyz);
+                std::string e = S->analyze(ndof, cp, ri, 3, hsp, descr, xyz);
                 if (e.empty())
                     *out = std::move(S);
                 else
@@ -482,7 +500,48 @@ struct Forging3D {
         int dev = 0;
         cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
         const double *xyz = ordering == 1 ? node_xyz.data() : nullptr;
-        sym_job = std::thread([this, dev, xyz] { analysis_job(dev, xyz, &sym_pre, &sym_err); });
+        sym_job = std::thread([this, dev, xyz] { analysis_job(dev, &topo, xyz, &sym_pre, &sym_err); });
+    }
+
+    // The remesher's topology hook: the new mesh's topology and symbolic analysis on the job thread, while the
+    // remesher places and remaps. The analysis orders by the nodes' stuffed positions (the order only shapes the
+    // fill); set_mesh takes the topology when it is handed the same tets.
+    void start_ahead(const std::vector<d3> &x, const std::vector<int32_t> &t, const std::vector<uint8_t> &onx,
+                     const std::vector<uint8_t> &ony)
+    {
+        join_analysis();
+        sym_pre.reset();
+        sym_err.clear();
+        int dev = 0;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        ahead_x.resize(3 * x.size());
+        for (size_t n = 0; n < x.size(); n++) st3(ahead_x.data(), (int)n, x[n]);
+        ahead_t = t;
+        ahead_onx = onx;
+        ahead_ony = ony;
+        topo_ahead.reset(new TetTopology);
+        topo_promise = std::promise<std::string>();
+        topo_ready = topo_promise.get_future();
+        ahead_pending = true;
+        const bool xyz = ordering == 1;
+        sym_job = std::thread([this, dev, xyz] {
+            std::string e;
+            try {
+                e = topo_ahead->build((int)(ahead_x.size() / 3), (int)(ahead_t.size() / 4), ahead_x.data(),
+                                      ahead_t.data(), ahead_onx.data(), ahead_ony.data());
+            } catch (std::exception &x) {
+                e = x.what();
+            }
+            // the pattern's addresses are taken before set_mesh may swap the topology in (the buffers move with it)
+            const int ndof = topo_ahead->ndof;
+            const int32_t *cp = topo_ahead->col_ptr.data(), *ri = topo_ahead->row_idx.data();
+            topo_promise.set_value(e);
+            if (!e.empty()) {
+                sym_err = e;
+                return;
+            }
+            analysis_job(dev, ndof, cp, ri, xyz ? ahead_x.data() : nullptr, &sym_pre, &sym_err);
+        });
     }
 
     // the analysis for the next factorisation: the one started with the mesh when it is there, else made now
@@ -507,13 +566,29 @@ struct Forging3D {
 
     void set_mesh(int nn, int ne, const double *x, const int32_t *tets, const uint8_t *ox, const uint8_t *oy)
     {
-        join_analysis();
-        sym_pre.reset();
-        sym_err.clear();
-        std::string e = topo.build(nn, ne, x, tets, ox, oy);
-        if (!e.empty()) throw Failure(IFEA_INPUT_INVALID, e);
-        node_xyz.assign(x, x + 3 * (size_t)nn);
-        start_analysis();
+        // the topology built ahead for these tets (a remesh), its analysis still running; else both made here
+        bool ahead = ahead_pending && ahead_t.size() == 4 * (size_t)ne && ahead_x.size() == 3 * (size_t)nn &&
+                     std::equal(ahead_t.begin(), ahead_t.end(), tets) &&
+                     std::equal(ahead_onx.begin(), ahead_onx.end(), ox) && std::equal(ahead_ony.begin(), ahead_ony.end(), oy);
+        if (ahead) {
+            ahead_pending = false;
+            std::string e = topo_ready.get();
+            if (!e.empty()) {
+                join_analysis();
+                throw Failure(IFEA_INPUT_INVALID, e);
+            }
+            std::swap(topo, *topo_ahead);
+            node_xyz.assign(x, x + 3 * (size_t)nn);
+        } else {
+            join_analysis();
+            ahead_pending = false;
+            sym_pre.reset();
+            sym_err.clear();
+            std::string e = topo.build(nn, ne, x, tets, ox, oy);
+            if (!e.empty()) throw Failure(IFEA_INPUT_INVALID, e);
+            node_xyz.assign(x, x + 3 * (size_t)nn);
+            start_analysis();
+        }
         std::vector<double> hl = local_lengths(topo, x, h);
         d_tets.upload(topo.tets, st); d_nts.upload(topo.nts, st); d_ntl.upload(topo.ntl, st); d_qk.upload(topo.qk, st);
         d_gslot.upload(topo.gslot, st); d_bface.upload(topo.bface, st); d_bowner.upload(topo.bowner, st);
@@ -651,7 +726,7 @@ struct Forging3D {
             d_wsy2.resize((size_t)3 * nn);
             for (int p = 0; p < ws_smooth; p++) {
                 k_ws_smooth<<<grid(nn), 256, 0, st>>>(V, d_wsy, d_wsy2);
-                std::swap(d_wsy.p, d_wsy2.p);
+                swap_buf(d_wsy, d_wsy2);
             }
         }
         k_ws_guess<<<grid(nn), 256, 0, st>>>(V, d_wsv0, d_wsy, d_vbuf[1 - vcur]);
@@ -1026,8 +1101,8 @@ struct Forging3D {
             }
             return false;
         }
-        std::swap(d_x.p, d_xT.p);
-        std::swap(d_contact.p, d_cT.p);
+        swap_buf(d_x, d_xT);
+        swap_buf(d_contact, d_cT);
         gap = gapT;
         time += dt;
         return true;
@@ -1121,6 +1196,8 @@ struct Forging3D {
         in.gap = gap; in.h = h; in.vol_target = vol0 / P.sym_factor; in.sym_x = P.sym_x != 0; in.sym_y = P.sym_y != 0;
         in.recovery_pass = recovery_pass; in.refinement_levels = refinement_levels; in.max_nodes = max_nodes;
         in.sig_ref = sig_ref; in.hot = hot;
+        in.on_topology = [this](const std::vector<d3> &px, const std::vector<int32_t> &pt, const std::vector<uint8_t> &onx,
+                                const std::vector<uint8_t> &ony) { start_ahead(px, pt, onx, ony); };
         RemeshOutput out;
         if (!remesh_workpiece(in, out)) {
             remesh_rejected++;
