@@ -541,69 +541,106 @@ __device__ __forceinline__ void dev_wide_acc(Dev<T> D, int s, const T *y, int ch
     }
 }
 
-// The forward GEMVs with the row tile sized to the level: a CTA takes 32 RG rows (warp w: the 32 consecutive
-// rows of row group w % RG, i.e. 128 contiguous bytes of each FP32 column, and the columns w / RG, w / RG + CG,
-// ..., CG = 16 / RG), sixteen loads in flight per thread; the column groups' partial sums meet in shared memory
-// and are added in group order. RG grows as the level's pivot blocks narrow, so that a thread still has some
-// tens of loads to issue.
-template <typename T, int RG>
-__device__ __forceinline__ T rows_dot(const T *__restrict__ A, int64_t ld, int row, int nrows, int c_end,
-                                      const T *__restrict__ v, bool lower)
+// Mirror pass (end of a factorisation): every wide front's L21 is copied transposed into the front's unused upper
+// right block, F(k, nc + i) = L21(i, k), and its pivot-block inverse X into the unused upper triangle of its
+// storage, X(c, r) = X(r, c). The forward solve then reads a row of L21 or of X as one contiguous run (the same
+// access as the backward solve's columns). 32 x 32 tiles through shared memory; the wide fronts' tiles form one
+// sequence (front f owns tiles tstart[f] ..), L21's tiles before X's lower ones.
+template <typename T>
+static __global__ void __launch_bounds__(256) k_mirror(Dev<T> D, const int32_t *__restrict__ big,
+                                                       const int64_t *__restrict__ tstart, int nbig)
 {
-    constexpr int CG = 16 / RG;
-    const int cg = (threadIdx.x >> 5) / RG;
-    T acc = 0;
-    if (row < nrows) {
-        const int ce = lower ? min(c_end, row + 1) : c_end;
-#pragma unroll 16
-        for (int c = cg; c < ce; c += CG) acc = fma(A[(int64_t)c * ld + row], __ldg(v + c), acc);
+    __shared__ T tile[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int64_t total = tstart[nbig];
+    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
+        int lo = 0, hi = nbig - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (tstart[mid] <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        const int s = big[lo], ms = D.m[s], nc = D.ncol[s], nr = ms - nc;
+        int64_t t = g - tstart[lo];
+        const int tk = (nc + 31) >> 5, tl21 = ((nr + 31) >> 5) * tk;
+        if (t < tl21) {
+            // L21 rows i0 .., columns k0 ..: read along i (a column of the front), write along k
+            const int i0 = (int)(t / tk) * 32, k0 = (int)(t % tk) * 32;
+            T *F = D.F + D.front_off[s];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                int i = i0 + tx, k = k0 + ty + 8 * j;
+                tile[ty + 8 * j][tx] = (i < nr && k < nc) ? F[(int64_t)k * ms + nc + i] : T(0);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                int k = k0 + tx, i = i0 + ty + 8 * j;
+                if (i < nr && k < nc) F[(int64_t)(nc + i) * ms + k] = tile[tx][ty + 8 * j];
+            }
+        } else {
+            // X lower tile (rows r0 .., columns c0 .., r0 >= c0) into the upper triangle
+            t -= tl21;
+            int br = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+            while ((int64_t)(br + 1) * (br + 2) / 2 <= t) br++;
+            while ((int64_t)br * (br + 1) / 2 > t) br--;
+            const int bc = (int)(t - (int64_t)br * (br + 1) / 2), r0 = br * 32, c0 = bc * 32;
+            T *X = D.Xinv + D.xinv_off[s];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                int r = r0 + tx, c = c0 + ty + 8 * j;
+                tile[ty + 8 * j][tx] = (r < nc && c < nc && r > c) ? X[(int64_t)c * nc + r] : T(0);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                int c = c0 + tx, r = r0 + ty + 8 * j;
+                if (r < nc && c < nc && r > c) X[(int64_t)r * nc + c] = tile[tx][ty + 8 * j];
+            }
+        }
+        __syncthreads();
     }
+}
+
+// One row of a mirrored operand against a vector: warp-wide dot product over a contiguous run, sixteen loads in
+// flight per lane, lanes summed by a shuffle tree (fixed order).
+template <typename T>
+__device__ __forceinline__ T warp_dot(const T *__restrict__ row, const T *__restrict__ v, int len, int lane)
+{
+    T acc = 0;
+#pragma unroll 16
+    for (int c = lane; c < len; c += 32) acc = fma(row[c], __ldg(v + c), acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     return acc;
 }
 
-// y1 = X acc1 (X lower triangular), 32 RG rows per CTA, row tiles counted from the bottom (longest rows first)
-template <typename T, int RG>
-static __global__ void __launch_bounds__(512) k_wide_fwd_y2(Dev<T> D, const int32_t *__restrict__ fronts, T *y, T *Y1)
+// y1 = X acc1 (X lower triangular, read through its mirror: row r is X(c, r) for c <= r, contiguous), one warp
+// per row, 16 rows per CTA counted from the bottom (longest rows first)
+template <typename T>
+static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32_t *__restrict__ fronts, T *y, T *Y1)
 {
-    constexpr int RTT = 32 * RG, CG = 16 / RG;
-    __shared__ T part[CG][RTT];
     const int s = fronts[blockIdx.y];
-    const int nc = D.ncol[s], c0 = D.c0[s], ntile = (nc + RTT - 1) / RTT;
+    const int nc = D.ncol[s], c0 = D.c0[s], ntile = (nc + 15) / 16;
     if ((int)blockIdx.x >= ntile) return;
-    const int r0 = (ntile - 1 - blockIdx.x) * RTT, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rr = 32 * (warp % RG) + lane;
-    T v = rows_dot<T, RG>(D.Xinv + D.xinv_off[s], nc, r0 + rr, nc, min(nc, r0 + RTT), D.Abig + D.idx_start[s], true);
-    part[warp / RG][rr] = v;
-    __syncthreads();
-    if ((int)threadIdx.x < RTT && r0 + (int)threadIdx.x < nc) {
-        T t = 0;
-#pragma unroll
-        for (int q = 0; q < CG; q++) t += part[q][threadIdx.x];
-        y[c0 + r0 + threadIdx.x] = t;
-        Y1[D.idx_start[s] + r0 + threadIdx.x] = t;
+    const int r = (ntile - 1 - blockIdx.x) * 16 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (r >= nc) return;
+    const T v = warp_dot(D.Xinv + D.xinv_off[s] + (int64_t)r * nc, D.Abig + D.idx_start[s], r + 1, lane);
+    if (lane == 0) {
+        y[c0 + r] = v;
+        Y1[D.idx_start[s] + r] = v;
     }
 }
 
-// update vector t = -acc2 + L21 y1, 32 RG rows per CTA
-template <typename T, int RG>
-static __global__ void __launch_bounds__(512) k_wide_fwd_t2(Dev<T> D, const int32_t *__restrict__ fronts, const T *Y1)
+// update vector t = -acc2 + L21 y1 (L21 through its mirror: row i is F(k, nc + i), k < nc), one warp per row
+template <typename T>
+static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32_t *__restrict__ fronts, const T *Y1)
 {
-    constexpr int RTT = 32 * RG, CG = 16 / RG;
-    __shared__ T part[CG][RTT];
     const int s = fronts[blockIdx.y];
-    const int ms = D.m[s], nc = D.ncol[s], nr = ms - nc, i0 = blockIdx.x * RTT;
-    if (i0 >= nr) return;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, rr = 32 * (warp % RG) + lane;
-    T v = rows_dot<T, RG>(D.F + D.front_off[s] + nc, ms, i0 + rr, nr, nc, Y1 + D.idx_start[s], false);
-    part[warp / RG][rr] = v;
-    __syncthreads();
-    if ((int)threadIdx.x < RTT && i0 + (int)threadIdx.x < nr) {
-        T t = 0;
-#pragma unroll
-        for (int q = 0; q < CG; q++) t += part[q][threadIdx.x];
-        int ii = i0 + threadIdx.x;
-        D.U[D.uvec_start[s] + ii] = -D.Abig[D.idx_start[s] + nc + ii] + t;
-    }
+    const int ms = D.m[s], nc = D.ncol[s], nr = ms - nc;
+    const int i = blockIdx.x * 16 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= nr) return;
+    const T v = warp_dot(D.F + D.front_off[s] + (int64_t)(nc + i) * ms, Y1 + D.idx_start[s], nc, lane);
+    if (lane == 0) D.U[D.uvec_start[s] + i] = -D.Abig[D.idx_start[s] + nc + i] + v;
 }
 
 // z = y1 - L21^T x2, one warp per pivot column; x2 is read through the front's row indices as the column
@@ -1414,6 +1451,15 @@ public:
             std::stable_sort(big_list_.begin() + big_start_[l], big_list_.begin() + big_start_[l + 1],
                              [&](int a, int b) { return S.ncol[a] > S.ncol[b]; });
         d_big_.upload(big_list_, st_);
+        {
+            std::vector<int64_t> ts(big_list_.size() + 1, 0);
+            for (size_t q = 0; q < big_list_.size(); q++) {
+                int sn = big_list_[q], nc = S.ncol[sn], nr = S.m[sn] - nc, tk = (nc + 31) / 32, tr = (nr + 31) / 32;
+                ts[q + 1] = ts[q] + (int64_t)tr * tk + (int64_t)tk * (tk + 1) / 2;
+            }
+            mirror_tiles_ = ts.back();
+            d_mirror_ts_.upload(ts, st_);
+        }
         wide_smem_ = 8;
         for (int sn : big_list_) wide_smem_ = std::max(wide_smem_, (size_t)std::max(S.ncol[sn], S.m[sn] - S.ncol[sn]) * sizeof(T));
         if (wide_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the wide solve kernels' shared-memory window");
@@ -1635,6 +1681,9 @@ public:
             cuda_check(cudaEventRecord(join_ev_, side_), "cudaEventRecord");
             cuda_check(cudaStreamWaitEvent(st, join_ev_, 0), "cudaStreamWaitEvent");
         }
+        if (mirror_tiles_ > 0)
+            mf::k_mirror<T><<<(int)std::min<int64_t>(mirror_tiles_, 8 * 148), 256, 0, st>>>(dev_, d_big_.p, d_mirror_ts_.p,
+                                                                                      (int)big_list_.size());
         cuda_check(cudaGetLastError(), "multifrontal factorisation launch");
     }
 
@@ -1787,16 +1836,8 @@ public:
                     mnc = std::max(mnc, S.ncol[big_list_[q]]);
                     mnr = std::max(mnr, S.m[big_list_[q]] - S.ncol[big_list_[q]]);
                 }
-                // rows per CTA from the level's widest pivot block: 256 rows up to 200 columns ... 32 from 800 on
-                int rg = mnc <= 200 ? 8 : mnc <= 400 ? 4 : mnc <= 800 ? 2 : 1, rt = 32 * rg;
-                dim3 gy((mnc + rt - 1) / rt, bc), gt((mnr + rt - 1) / rt, bc);
-                const int32_t *bl = d_big_.p + b0;
-                switch (rg) {
-                case 8: mf::k_wide_fwd_y2<T, 8><<<gy, 512, 0, st>>>(dev_, bl, d_y_, d_y1_); mf::k_wide_fwd_t2<T, 8><<<gt, 512, 0, st>>>(dev_, bl, d_y1_); break;
-                case 4: mf::k_wide_fwd_y2<T, 4><<<gy, 512, 0, st>>>(dev_, bl, d_y_, d_y1_); mf::k_wide_fwd_t2<T, 4><<<gt, 512, 0, st>>>(dev_, bl, d_y1_); break;
-                case 2: mf::k_wide_fwd_y2<T, 2><<<gy, 512, 0, st>>>(dev_, bl, d_y_, d_y1_); mf::k_wide_fwd_t2<T, 2><<<gt, 512, 0, st>>>(dev_, bl, d_y1_); break;
-                default: mf::k_wide_fwd_y2<T, 1><<<gy, 512, 0, st>>>(dev_, bl, d_y_, d_y1_); mf::k_wide_fwd_t2<T, 1><<<gt, 512, 0, st>>>(dev_, bl, d_y1_); break;
-                }
+                mf::k_wide_fwd_y<T><<<dim3((mnc + 15) / 16, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
+                mf::k_wide_fwd_t<T><<<dim3((mnr + 15) / 16, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
             }
         }
         for (int l = S.nlevels - 1; l >= 0; l--) {
@@ -1862,6 +1903,8 @@ private:
     static constexpr int kXinvChunk = 4;  // tile steps per CTA before a block range is split
     size_t small_smem_ = 8, wide_smem_ = 8, level_smem_ = 8;
     DBuf<int64_t> d_inv_off_, d_xinv_off_;
+    DBuf<int64_t> d_mirror_ts_;   // the wide fronts' mirror tiles, prefix per front
+    int64_t mirror_tiles_ = 0;
     DBuf<int32_t> d_small_, d_big_, d_gst_, d_gsrc_;
     DBuf<T> d_Inv_, d_Xinv_, d_Abig_, d_y1_, d_z_;
     cusparseMatDescr_t descr_ = nullptr;
