@@ -88,6 +88,8 @@ SIGNATURES = {
     "ifea3d_last_error": (C.c_char_p, [_vp]),
     "ifea3d_set_mesh": (_st, [_vp, C.c_int32, C.c_int32, _dp, _i32p, _u8p, _u8p]),
     "ifea3d_set_die": (_st, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, _dp]),
+    "ifea3d_set_trimesh_die": (_st, [_vp, C.c_int32, C.c_int32, _dp, C.c_int32, _i32p]),
+    "ifea3d_die_query": (_st, [_vp, C.c_int32, C.c_int32, _dp, C.c_double, _dp, _dp, _dp, _dp]),
     "ifea3d_init": (_st, [_vp] + [C.c_double] * 6),
     "ifea3d_step": (_st, [_vp, C.POINTER(StepInfo), _i32p]),
     "ifea3d_pattern_size": (_st, [_vp, _i64p, _i32p]),

@@ -207,10 +207,13 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
                         }
                         const double lkk = sqrt(piv);
                         if (lane == cc) v[0][cc] = lkk;
+                        // the quotients for every lane and row (no branch around the divisions, which would
+                        // serialise them), kept where the row belongs to column c's band
 #pragma unroll
                         for (int q = 0; q < kBlkRows; q++) {
                             int r = J + lane + 32 * q;
-                            if (r > c && r < R && r - c <= b) v[q][cc] = v[q][cc] / lkk;
+                            const double qv = v[q][cc] / lkk;
+                            if (r > c && r < R && r - c <= b) v[q][cc] = qv;
                         }
 #pragma unroll
                         for (int c2 = 0; c2 < 8; c2++) {
@@ -405,7 +408,8 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
             const int np = k1 - k0;
             double y = lane < np ? RV(k0 + lane) : 0.0;
             for (int kk = 0; kk < np; kk++) {
-                if (lane == kk) y = y / P(k0 + kk, k0 + kk);
+                const double yd = y / P(k0 + kk, k0 + kk);  // every lane divides; lane kk keeps it
+                if (lane == kk) y = yd;
                 double xk = __shfl_sync(FULL, y, kk);
                 if (lane > kk && lane < np && lane - kk <= b) y = y - P(k0 + lane, k0 + kk) * xk;
             }
@@ -451,7 +455,8 @@ __global__ void __launch_bounds__(kThreads) k_band_chol(int n, int b, int nb, in
             for (int kk = np - 1; kk >= 0; kk--) {
                 double en = 0.0;
                 if (kk >= 1 && lane < kk - 1 && kk - 1 - lane <= b) en = win[brow[kk - 1] + i0 + lane];
-                if (lane == kk) y = y / d;
+                const double yd = y / d;  // every lane divides; lane kk keeps it
+                if (lane == kk) y = yd;
                 const double xi = __shfl_sync(FULL, y, kk);
                 if (lane < kk && kk - lane <= b) y = y - e * xi;
                 e = en;

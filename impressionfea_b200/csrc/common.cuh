@@ -74,16 +74,140 @@ IFEA_HD double tet_quality(d3 a, d3 b, d3 c, d3 d)
 }
 
 // Rigid die z = h(x, y) on a regular grid (ThreeD/HeightFieldDie.cs). Pointer h lives in device memory.
+// A die given as a closed triangulated solid (TriMeshDie over TriMeshSolid, ThreeD/TriMeshSolid.cs:5-180, :248-297):
+// vertices, triangles, bounding box, and the solid's two bucket grids in its own layout (an xy grid of cell c2 for
+// vertical hits, a 3D grid of cell c3 for closest points; each cell lists its triangles in ascending order).
+struct TriGrid {
+    const double *v = nullptr;   // 3 per vertex
+    const int32_t *t = nullptr;  // 3 per triangle
+    int nt = 0;
+    double mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
+    double c2 = 1;
+    int nx2 = 1, ny2 = 1;
+    const int32_t *xy_start = nullptr, *xy_items = nullptr;
+    double c3 = 1;
+    int gx = 1, gy = 1, gz = 1;
+    const int32_t *g3_start = nullptr, *g3_items = nullptr;
+};
+
 struct HField {
     int side;  // 0 bottom, 1 top
     int nx, ny;
     double x0, y0, dx;
     const double *h;
+    int kind = 0;  // 0 height field (the fields above), 1 triangulated solid (tm)
+    TriGrid tm;
 };
 
-// HeightAt (:100-107)
+IFEA_HD d3 tm_vertex(const TriGrid &g, int i) { return mk3(g.v[3 * i], g.v[3 * i + 1], g.v[3 * i + 2]); }
+
+// VerticalHits (TriMeshSolid.cs:96-121): every triangle of the point's xy cell that the vertical line through the
+// (jittered) point crosses, as its z; visit(z) for each.
+template <typename F>
+IFEA_HD void tm_vertical_hits(const TriGrid &g, double x, double y, F &&visit)
+{
+    if (x < g.mn[0] || x > g.mx[0] || y < g.mn[1] || y > g.mx[1]) return;
+    x += 1.2345e-7;
+    y += 2.3456e-7;
+    int cx = iclamp((int)((x - g.mn[0]) / g.c2), 0, g.nx2 - 1), cy = iclamp((int)((y - g.mn[1]) / g.c2), 0, g.ny2 - 1);
+    int cell = cy * g.nx2 + cx;
+    for (int q = g.xy_start[cell]; q < g.xy_start[cell + 1]; q++) {
+        int t = g.xy_items[q];
+        d3 a = tm_vertex(g, g.t[3 * t]), b = tm_vertex(g, g.t[3 * t + 1]), c = tm_vertex(g, g.t[3 * t + 2]);
+        double d = (b.x - a.x) * (c.y - a.y) - (c.x - a.x) * (b.y - a.y);
+        if (fabs(d) < 1e-300) continue;
+        double u = ((x - a.x) * (c.y - a.y) - (c.x - a.x) * (y - a.y)) / d;
+        double v = ((b.x - a.x) * (y - a.y) - (x - a.x) * (b.y - a.y)) / d;
+        if (u < 0 || v < 0 || u + v > 1) continue;
+        visit(a.z + u * (b.z - a.z) + v * (c.z - a.z));
+    }
+}
+
+// Contains (:125-137): inside when an odd number of hits lies above the point
+IFEA_HD bool tm_contains(const TriGrid &g, d3 p)
+{
+    if (p.x < g.mn[0] || p.x > g.mx[0] || p.y < g.mn[1] || p.y > g.mx[1] || p.z < g.mn[2] || p.z > g.mx[2]) return false;
+    int above = 0;
+    tm_vertical_hits(g, p.x, p.y, [&](double z) { above += z > p.z; });
+    return (above & 1) == 1;
+}
+
+// Closest (:139-178): rings of 3D cells around the point's cell until the best distance is within the ring
+IFEA_HD bool tm_closest(const TriGrid &g, d3 p, double maxd, d3 *point, d3 *normal, double *dist)
+{
+    d3 bp = p, bn = mk3(0, 0, 1);
+    int ci = (int)floor((p.x - g.mn[0]) / g.c3), cj = (int)floor((p.y - g.mn[1]) / g.c3), ck = (int)floor((p.z - g.mn[2]) / g.c3);
+    int max_ring = (int)ceil(maxd / g.c3) + 1;
+    double best = maxd * maxd;
+    for (int ring = 0; ring <= max_ring; ring++) {
+        for (int k = ck - ring; k <= ck + ring; k++) {
+            if (k < 0 || k >= g.gz) continue;
+            for (int j = cj - ring; j <= cj + ring; j++) {
+                if (j < 0 || j >= g.gy) continue;
+                bool shell_row = abs(j - cj) == ring || abs(k - ck) == ring;
+                int istep = shell_row || ring == 0 ? 1 : 2 * ring;
+                for (int i = ci - ring; i <= ci + ring; i += istep) {
+                    if (i < 0 || i >= g.gx) continue;
+                    int cell = (k * g.gy + j) * g.gx + i;
+                    for (int q = g.g3_start[cell]; q < g.g3_start[cell + 1]; q++) {
+                        int t = g.g3_items[q];
+                        d3 a = tm_vertex(g, g.t[3 * t]), b = tm_vertex(g, g.t[3 * t + 1]), c = tm_vertex(g, g.t[3 * t + 2]);
+                        d3 cq = closest_on_triangle(p, a, b, c);
+                        double dd = len23(sub3(cq, p));
+                        if (dd >= best) continue;
+                        best = dd;
+                        bp = cq;
+                        bn = nrm3(cross3(sub3(b, a), sub3(c, a)));
+                    }
+                }
+            }
+        }
+        if (sqrt(best) <= ring * g.c3) break;
+    }
+    *point = bp;
+    *normal = bn;
+    *dist = sqrt(best);
+    return *dist < maxd;
+}
+
+// TriMeshDie.Clearance / Project / SurfaceZ (:267-296): the die moved by `offset` along z; Reach = 6 mm
+IFEA_HD double tm_clearance(const TriGrid &g, d3 p, double offset)
+{
+    const double reach = 6;
+    d3 q = mk3(p.x, p.y, p.z - offset);
+    if (q.x < g.mn[0] - reach || q.x > g.mx[0] + reach || q.y < g.mn[1] - reach || q.y > g.mx[1] + reach ||
+        q.z < g.mn[2] - reach || q.z > g.mx[2] + reach)
+        return reach;
+    bool inside = tm_contains(g, q);
+    d3 c, n;
+    double dist;
+    double d = tm_closest(g, q, reach, &c, &n, &dist) ? dist : reach;
+    return inside ? -d : d;
+}
+IFEA_HD d3 tm_project(const TriGrid &g, int side, d3 p, double offset, d3 *normal)
+{
+    const double reach = 6;
+    d3 q = mk3(p.x, p.y, p.z - offset), c, n;
+    double dist;
+    if (!tm_closest(g, q, 4 * reach, &c, &n, &dist)) n = side == 0 ? mk3(0, 0, 1) : mk3(0, 0, -1);
+    if (normal) *normal = n;
+    return mk3(c.x, c.y, c.z + offset);
+}
+IFEA_HD double tm_surface_z(const TriGrid &g, int side, double x, double y)
+{
+    bool any = false;
+    double z = 0;
+    tm_vertical_hits(g, x, y, [&](double h) {
+        z = !any ? h : (side == 0 ? rmax(z, h) : rmin(z, h));
+        any = true;
+    });
+    return any ? z : NAN;
+}
+
+// HeightAt (:100-107); a triangulated die's SurfaceZ
 IFEA_HD double hf_height(const HField &d, double x, double y)
 {
+    if (d.kind == 1) return tm_surface_z(d.tm, d.side, x, y);
     double fx = rclamp((x - d.x0) / d.dx, 0, d.nx), fy = rclamp((y - d.y0) / d.dx, 0, d.ny);
     int i = min((int)fx, d.nx - 1), j = min((int)fy, d.ny - 1);
     double u = fx - i, v = fy - j;
@@ -95,6 +219,7 @@ IFEA_HD double hf_height(const HField &d, double x, double y)
 // Clearance (:130-134): > 0 in the open cavity, < 0 penetrating.
 IFEA_HD double hf_clearance(const HField &d, d3 p, double offset)
 {
+    if (d.kind == 1) return tm_clearance(d.tm, p, offset);
     double h = hf_height(d, p.x, p.y) + offset;
     return d.side == 0 ? p.z - h : h - p.z;
 }
@@ -107,6 +232,7 @@ IFEA_HD d3 hf_vertex(const HField &d, int i, int j, double offset)
 // Project (:157-191): closest point over the two triangles of each cell within reach; normal out of the die.
 IFEA_HD d3 hf_project(const HField &d, d3 p, double offset, d3 *normal)
 {
+    if (d.kind == 1) return tm_project(d.tm, d.side, p, offset, normal);
     double reach = fabs(hf_clearance(d, p, offset)) + 1.5 * d.dx;
     int i0 = iclamp((int)floor((p.x - reach - d.x0) / d.dx), 0, d.nx - 1);
     int i1 = iclamp((int)floor((p.x + reach - d.x0) / d.dx), 0, d.nx - 1);

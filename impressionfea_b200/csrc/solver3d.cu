@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "remesh.h"
+#include "trimesh.h"
 #include "warmstart.h"
 #include "kernels3d.cuh"
 #include "mesh3d.h"
@@ -246,6 +247,18 @@ struct PhaseTimer {
     ~PhaseTimer() { acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
 };
 
+__global__ void k_die_query(HField d, int n, const double *p, double offset, double *out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        d3 q = ld3(p, i), nrm;
+        double *o = out + 8 * (size_t)i;
+        o[0] = hf_clearance(d, q, offset);
+        d3 r = hf_project(d, q, offset, &nrm);
+        o[1] = r.x, o[2] = r.y, o[3] = r.z, o[4] = nrm.x, o[5] = nrm.y, o[6] = nrm.z;
+        o[7] = hf_height(d, q.x, q.y);
+    }
+}
+
 struct Forging3D {
     ifea3d_params P;
     double t_trigger = 0, t_prepare = 0, t_assemble = 0, t_linesearch = 0, t_factor = 0, t_pcg = 0, t_final = 0,
@@ -307,6 +320,9 @@ struct Forging3D {
     d3 fail_at = mk3(0, 0, 0);
     bool have_fail_at = false;
     std::vector<double> die_host[2];  // host copies of the die heights (the remesher's clearances)
+    TriMeshHost tm_host[2];            // triangulated dies: host grids (the remesher's), device copies below
+    DBuf<double> tm_v[2];
+    DBuf<int32_t> tm_t[2], tm_xys[2], tm_xyi[2], tm_g3s[2], tm_g3i[2];
     std::string last_remesh;
     DBuf<double> d_cavity;          // the closed cavity's sample points (FillPercent)
     DBuf<int32_t> d_loc_start, d_loc_fill, d_loc_items;
@@ -637,6 +653,52 @@ struct Forging3D {
         cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
     }
 
+    // a die given as a closed triangulated solid (TriMeshDie, ThreeD/TriMeshSolid.cs:248-297), in its closed
+    // position for the top die like the height field
+    void set_trimesh_die(int side, int nv, const double *v, int nt, const int32_t *tri)
+    {
+        if (side < 0 || side > 1) throw Failure(IFEA_INPUT_INVALID, "invalid die side");
+        TriMeshHost &h = tm_host[side];
+        std::string e = h.build(nv, v, nt, tri);
+        if (!e.empty()) throw Failure(IFEA_INPUT_INVALID, e);
+        tm_v[side].upload(h.v, st); tm_t[side].upload(h.t, st);
+        tm_xys[side].upload(h.xy_start, st); tm_xyi[side].upload(h.xy_items.empty() ? std::vector<int32_t>{0} : h.xy_items, st);
+        tm_g3s[side].upload(h.g3_start, st); tm_g3i[side].upload(h.g3_items.empty() ? std::vector<int32_t>{0} : h.g3_items, st);
+        HField &d = die[side];
+        d.side = side;
+        d.kind = 1;
+        d.nx = d.ny = 1;
+        d.x0 = h.grid.mn[0]; d.y0 = h.grid.mn[1]; d.dx = h.grid.c2;
+        d.h = nullptr;
+        d.tm = h.grid;
+        d.tm.v = tm_v[side].p; d.tm.t = tm_t[side].p;
+        d.tm.xy_start = tm_xys[side].p; d.tm.xy_items = tm_xyi[side].p;
+        d.tm.g3_start = tm_g3s[side].p; d.tm.g3_items = tm_g3i[side].p;
+        die_host[side].clear();
+        have_dies |= 1 << side;
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    }
+
+    // Clearance, Project and SurfaceZ of one die at n points, on the device (the queries the increment uses)
+    void die_query(int side, int n, const double *p, double offset, double *clr, double *proj, double *nrm, double *sz)
+    {
+        if (side < 0 || side > 1 || !(have_dies & (1 << side))) throw Failure(IFEA_BAD_STATE, "that die is not set");
+        if (n == 0) return;
+        DBuf<double> dp, dout;
+        dp.upload(p, 3 * (size_t)n, st);
+        dout.resize(8 * (size_t)n);
+        k_die_query<<<grid(n), 256, 0, st>>>(die[side], n, dp.p, offset, dout.p);
+        cuda_check(cudaGetLastError(), "k_die_query");
+        std::vector<double> o(8 * (size_t)n);
+        dout.download(o.data(), o.size(), st);
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        for (int i = 0; i < n; i++) {
+            clr[i] = o[8 * (size_t)i];
+            for (int a = 0; a < 3; a++) proj[3 * (size_t)i + a] = o[8 * (size_t)i + 1 + a], nrm[3 * (size_t)i + a] = o[8 * (size_t)i + 4 + a];
+            sz[i] = o[8 * (size_t)i + 7];
+        }
+    }
+
     void set_die(int side, int nx, int ny, double x0, double y0, double dx, const double *hh)
     {
         if (side < 0 || side > 1 || nx < 1 || ny < 1 || !(dx > 0)) throw Failure(IFEA_INPUT_INVALID, "invalid die grid");
@@ -644,6 +706,7 @@ struct Forging3D {
         die_host[side].assign(hh, hh + (size_t)(nx + 1) * (ny + 1));
         die[side].side = side; die[side].nx = nx; die[side].ny = ny;
         die[side].x0 = x0; die[side].y0 = y0; die[side].dx = dx; die[side].h = die_h[side].p;
+        die[side].kind = 0;
         have_dies |= 1 << side;
         cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
     }
@@ -1175,7 +1238,7 @@ struct Forging3D {
     bool remesh(const std::string &reason)
     {
         PhaseTimer pt(t_remesh);
-        if (die_host[0].empty() || die_host[1].empty()) throw Failure(IFEA_BAD_STATE, "remeshing needs both dies");
+        if (have_dies != 3) throw Failure(IFEA_BAD_STATE, "remeshing needs both dies");
         size_t nn = topo.nn, ne = topo.ne;
         std::vector<double> x(3 * nn), vg(3 * nn), eps(ne), dmg(ne), sig(ne), rate(ne), mean(ne);
         d_x.download(x.data(), 3 * nn, st);
@@ -1191,7 +1254,8 @@ struct Forging3D {
         in.eps = eps.data(); in.dmg = dmg.data(); in.sig = sig.data(); in.rate = rate.data(); in.mean = mean.data();
         for (int k = 0; k < 2; k++) {
             in.die[k] = die[k];
-            in.die[k].h = die_host[k].data();
+            if (die[k].kind == 1) in.die[k].tm = tm_host[k].grid;  // host copies of the grids
+            else in.die[k].h = die_host[k].data();
         }
         in.gap = gap; in.h = h; in.vol_target = vol0 / P.sym_factor; in.sym_x = P.sym_x != 0; in.sym_y = P.sym_y != 0;
         in.recovery_pass = recovery_pass; in.refinement_levels = refinement_levels; in.max_nodes = max_nodes;
@@ -1525,6 +1589,19 @@ ifea_status ifea3d_set_die(ifea3d *ctx, int32_t side, int32_t nx, int32_t ny, do
 {
     if (!h) return IFEA_INPUT_INVALID;
     return guarded(ctx, [&](Forging3D &s) { s.set_die(side, nx, ny, x0, y0, dx, h); });
+}
+
+ifea_status ifea3d_set_trimesh_die(ifea3d *ctx, int32_t side, int32_t nv, const double *v, int32_t nt, const int32_t *tri)
+{
+    if (!v || !tri) return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) { s.set_trimesh_die(side, nv, v, nt, tri); });
+}
+
+ifea_status ifea3d_die_query(ifea3d *ctx, int32_t side, int32_t n, const double *p, double offset, double *clearance,
+                             double *projected, double *normal, double *surface_z)
+{
+    if (n < 0 || (n > 0 && (!p || !clearance || !projected || !normal || !surface_z))) return IFEA_INPUT_INVALID;
+    return guarded(ctx, [&](Forging3D &s) { s.die_query(side, n, p, offset, clearance, projected, normal, surface_z); });
 }
 
 ifea_status ifea3d_init(ifea3d *ctx, double gap0, double min_x, double min_y, double min_z, double max_x, double max_y)

@@ -33,8 +33,13 @@ class Forging3DSolver:
         oy = np.ascontiguousarray(mesh.on_y0, np.uint8)
         self._check(L.ifea3d_set_mesh(h, len(x), len(t), _dp(x), _ip(t), _u8(ox), _u8(oy)))
         for side, d in enumerate(dies):
-            hh = np.ascontiguousarray(d.h, np.float64)
-            self._check(L.ifea3d_set_die(h, side, d.nx, d.ny, d.x0, d.y0, d.dx, _dp(hh)))
+            if hasattr(d, "triangles"):
+                v = np.ascontiguousarray(d.vertices, np.float64)
+                t = np.ascontiguousarray(d.triangles, np.int32)
+                self._check(L.ifea3d_set_trimesh_die(h, side, len(v), _dp(v), len(t), _ip(t)))
+            else:
+                hh = np.ascontiguousarray(d.h, np.float64)
+                self._check(L.ifea3d_set_die(h, side, d.nx, d.ny, d.x0, d.y0, d.dx, _dp(hh)))
         self._check(L.ifea3d_init(h, mesh.gap0, *mesh.bounds_for_velocity))
         self.nn, self.ne = len(x), len(t)
         self.last_info = None
@@ -158,6 +163,15 @@ class Forging3DSolver:
         v = C.c_double()
         self._check(self._L.ifea3d_get_scalar(self._h, name.encode(), C.byref(v)))
         return v.value
+
+    def die_query(self, side, points, offset=0.0):
+        """Clearance, projection, normal and surface height of die `side` (moved by offset along z) at points
+        (n, 3), evaluated on the device: returns (clearance[n], projected[n,3], normal[n,3], surface_z[n])."""
+        p = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+        n = len(p)
+        c, q, nr, z = np.zeros(n), np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n)
+        self._check(self._L.ifea3d_die_query(self._h, int(side), n, _dp(p), float(offset), _dp(c), _dp(q), _dp(nr), _dp(z)))
+        return c, q, nr, z
 
     def set_scalar(self, name, value):
         self._check(self._L.ifea3d_set_scalar(self._h, name.encode(), float(value)))

@@ -64,6 +64,52 @@ class HeightField:
         return HeightField(x0, y0, dx, nx, ny, np.ascontiguousarray(fn(X, Y), np.float64).ravel())
 
 
+@dataclass
+class TriMeshDie:
+    """Rigid die as a closed triangulated solid (TriMeshDie over TriMeshSolid, ThreeD/TriMeshSolid.cs:248-297):
+    vertices (nv, 3), triangles (nt, 3) wound with outward normals; the top die given in its closed position."""
+    vertices: np.ndarray
+    triangles: np.ndarray
+
+    @staticmethod
+    def box(lo, hi):
+        """An axis-aligned box (12 triangles, outward winding)."""
+        (x0, y0, z0), (x1, y1, z1) = lo, hi
+        v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                      [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]], np.float64)
+        t = np.array([[0, 2, 1], [0, 3, 2], [4, 5, 6], [4, 6, 7], [0, 1, 5], [0, 5, 4],
+                      [1, 2, 6], [1, 6, 5], [2, 3, 7], [2, 7, 6], [3, 0, 4], [3, 4, 7]], np.int32)
+        return TriMeshDie(v, t)
+
+    @staticmethod
+    def grid_block(fn, x0, x1, y0, y1, n, z_far, top):
+        """A solid bounded by the surface z = fn(x, y) sampled on an (n+1) x (n+1) grid and the plane z = z_far
+        (below the surface for a bottom die, above it for a top die), closed by four side walls."""
+        xs, ys = np.linspace(x0, x1, n + 1), np.linspace(y0, y1, n + 1)
+        X, Y = np.meshgrid(xs, ys)
+        Z = np.asarray(fn(X, Y), np.float64)
+        m = (n + 1) * (n + 1)
+        top_v = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+        far_v = np.stack([X.ravel(), Y.ravel(), np.full(m, float(z_far))], 1)
+        v = np.concatenate([top_v, far_v])
+        idx = lambda i, j: j * (n + 1) + i
+        tris = []
+        for j in range(n):
+            for i in range(n):
+                a, b, c, d = idx(i, j), idx(i + 1, j), idx(i + 1, j + 1), idx(i, j + 1)
+                tris += [[a, b, c], [a, c, d]]                      # working surface, normal +z
+                tris += [[m + a, m + c, m + b], [m + a, m + d, m + c]]  # far plane, normal -z
+        ring = [idx(i, 0) for i in range(n)] + [idx(n, j) for j in range(n)] + \
+               [idx(i, n) for i in range(n, 0, -1)] + [idx(0, j) for j in range(n, 0, -1)]
+        for k in range(len(ring)):
+            p, q = ring[k], ring[(k + 1) % len(ring)]
+            tris += [[p, m + p, m + q], [p, m + q, q]]              # side walls, outward
+        t = np.array(tris, np.int32)
+        if top:  # the solid lies above its working surface: flip every triangle
+            t = t[:, [0, 2, 1]]
+        return TriMeshDie(v, t)
+
+
 def _quarter_disk_points(R, h):
     """Boundary nodes (on x=0, y=0 and the arc) and hexagonal-lattice interior nodes of the quarter disk."""
     n_edge = max(2, int(round(R / h)))

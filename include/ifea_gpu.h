@@ -101,6 +101,16 @@ ifea_status ifea3d_set_die(ifea3d *ctx, int32_t side, int32_t nx, int32_t ny, do
 
 /* Constructor tail (Forging3DSolver.cs:156-184): initial gap, initial contact and placement, initial velocity
  * from the billet bounds (min_x, min_y, min_z, max_x, max_y), reference volume. */
+/* A die given as a closed triangulated solid instead of a height field (TriMeshDie over TriMeshSolid,
+ * ThreeD/TriMeshSolid.cs:248-297): nv vertices (3 doubles each), nt triangles (3 vertex indices each, outward normals
+ * by winding), the top die in its closed position. Its clearance, projection and surface height follow the
+ * reference's bucket grids and ring search. */
+ifea_status ifea3d_set_trimesh_die(ifea3d *ctx, int32_t side, int32_t nv, const double *v, int32_t nt, const int32_t *tri);
+/* Clearance (IRigidDie.Clearance), Project (closest point, normal out of the die) and SurfaceZ of one die, moved by
+ * `offset` along z, at n points (3 doubles each), evaluated on the device: clearance[n], projected[3n], normal[3n],
+ * surface_z[n] (NaN where a triangulated die has no surface above or below the point). */
+ifea_status ifea3d_die_query(ifea3d *ctx, int32_t side, int32_t n, const double *p, double offset, double *clearance,
+                             double *projected, double *normal, double *surface_z);
 ifea_status ifea3d_init(ifea3d *ctx, double gap0, double min_x, double min_y, double min_z, double max_x,
                         double max_y);
 

@@ -136,6 +136,8 @@ double o2d_scalar(o2d *s, const char *name);
 double o2d_die_project(const double *pts, int npts, int side, double px, double py, double offset,
                        double *qx, double *qy, double *nx, double *ny);
 double o2d_die_height(const double *pts, int npts, double x);
+int o3d_set_trimesh_die(o3d *s, int side, int nv, const double *v, int nt, const int *tri);
+double o3d_die_height(o3d *s, int side, double x, double y);
 double o3d_die_project(o3d *s, int side, const double *p, double offset, double *q, double *nrm);
 double o3d_die_clearance(o3d *s, int side, const double *p, double offset);
 double o3d_tet_quality(const double *a, const double *b, const double *c, const double *d);

@@ -68,8 +68,186 @@ double o_principal_max3(double xx, double yy, double zz, double xy, double yz, d
 /* ------------------------------------------------------------------ height-field die */
 
 /* ThreeD/HeightFieldDie.cs:100-107 */
+/* ---- TriMeshSolid (ThreeD/TriMeshSolid.cs:17-82): bucket grids, each cell's triangles in ascending order ---- */
+void o_trimesh_free(o_trimesh *m)
+{
+    free(m->v); free(m->t); free(m->xy_start); free(m->xy_items); free(m->g3_start); free(m->g3_items);
+    memset(m, 0, sizeof *m);
+}
+
+static int tm_cx2(const o_trimesh *m, double x) { return iclamp((int)((x - m->mn[0]) / m->c2), 0, m->nx2 - 1); }
+static int tm_cy2(const o_trimesh *m, double y) { return iclamp((int)((y - m->mn[1]) / m->c2), 0, m->ny2 - 1); }
+static int tm_c3(const o_trimesh *m, double v, double lo, int n) { return iclamp((int)((v - lo) / m->c3), 0, n - 1); }
+
+int o_trimesh_build(o_trimesh *m, int nv, const double *v, int nt, const int *tri)
+{
+    o_trimesh_free(m);
+    if (nv < 3 || nt < 1) return -1;
+    for (int k = 0; k < 3 * nt; k++)
+        if (tri[k] < 0 || tri[k] >= nv) return -1;
+    m->nv = nv; m->nt = nt;
+    m->v = (double *)malloc(sizeof(double) * 3 * (size_t)nv);
+    m->t = (int *)malloc(sizeof(int) * 3 * (size_t)nt);
+    memcpy(m->v, v, sizeof(double) * 3 * (size_t)nv);
+    memcpy(m->t, tri, sizeof(int) * 3 * (size_t)nt);
+    for (int a = 0; a < 3; a++) m->mn[a] = DBL_MAX, m->mx[a] = -DBL_MAX;
+    for (int i = 0; i < nv; i++)
+        for (int a = 0; a < 3; a++) {
+            m->mn[a] = fmin(m->mn[a], v[3 * i + a]);
+            m->mx[a] = fmax(m->mx[a], v[3 * i + a]);
+        }
+    double ex = m->mx[0] - m->mn[0], ey = m->mx[1] - m->mn[1], ez = m->mx[2] - m->mn[2];
+    double ext = fmax(ex, fmax(ey, ez));
+    m->c2 = fmax(ext / 200, sqrt((ex + 1e-9) * (ey + 1e-9) / imax(nt, 1)) * 2);
+    m->nx2 = imax(1, (int)ceil(ex / m->c2) + 1);
+    m->ny2 = imax(1, (int)ceil(ey / m->c2) + 1);
+    m->c3 = fmax(ext / 120, cbrt((ex + 1e-9) * (ey + 1e-9) * (ez + 1e-9) / imax(nt, 1)) * 2);
+    m->gx = imax(1, (int)ceil(ex / m->c3) + 1);
+    m->gy = imax(1, (int)ceil(ey / m->c3) + 1);
+    m->gz = imax(1, (int)ceil(ez / m->c3) + 1);
+    size_t n2 = (size_t)m->nx2 * m->ny2, n3 = (size_t)m->gx * m->gy * m->gz;
+    m->xy_start = (int *)calloc(n2 + 1, sizeof(int));
+    m->g3_start = (int *)calloc(n3 + 1, sizeof(int));
+    int *f2 = NULL, *f3 = NULL;
+    for (int pass = 0; pass < 2; pass++) {
+        if (pass == 1) {
+            for (size_t c = 0; c < n2; c++) m->xy_start[c + 1] += m->xy_start[c];
+            for (size_t c = 0; c < n3; c++) m->g3_start[c + 1] += m->g3_start[c];
+            m->xy_items = (int *)malloc(sizeof(int) * (size_t)(m->xy_start[n2] + 1));
+            m->g3_items = (int *)malloc(sizeof(int) * (size_t)(m->g3_start[n3] + 1));
+            f2 = (int *)malloc(sizeof(int) * n2);
+            f3 = (int *)malloc(sizeof(int) * n3);
+            memcpy(f2, m->xy_start, sizeof(int) * n2);
+            memcpy(f3, m->g3_start, sizeof(int) * n3);
+        }
+        for (int k = 0; k < nt; k++) {
+            const double *a = m->v + 3 * m->t[3 * k], *b = m->v + 3 * m->t[3 * k + 1], *c = m->v + 3 * m->t[3 * k + 2];
+            double lx = fmin(a[0], fmin(b[0], c[0])), hx = fmax(a[0], fmax(b[0], c[0]));
+            double ly = fmin(a[1], fmin(b[1], c[1])), hy = fmax(a[1], fmax(b[1], c[1]));
+            double lz = fmin(a[2], fmin(b[2], c[2])), hz = fmax(a[2], fmax(b[2], c[2]));
+            for (int j = tm_cy2(m, ly); j <= tm_cy2(m, hy); j++)
+                for (int i = tm_cx2(m, lx); i <= tm_cx2(m, hx); i++) {
+                    size_t cell = (size_t)j * m->nx2 + i;
+                    if (pass == 0) m->xy_start[cell + 1]++;
+                    else m->xy_items[f2[cell]++] = k;
+                }
+            for (int kk = tm_c3(m, lz, m->mn[2], m->gz); kk <= tm_c3(m, hz, m->mn[2], m->gz); kk++)
+                for (int j = tm_c3(m, ly, m->mn[1], m->gy); j <= tm_c3(m, hy, m->mn[1], m->gy); j++)
+                    for (int i = tm_c3(m, lx, m->mn[0], m->gx); i <= tm_c3(m, hx, m->mn[0], m->gx); i++) {
+                        size_t cell = ((size_t)kk * m->gy + j) * m->gx + i;
+                        if (pass == 0) m->g3_start[cell + 1]++;
+                        else m->g3_items[f3[cell]++] = k;
+                    }
+        }
+    }
+    free(f2);
+    free(f3);
+    return 0;
+}
+
+static v3 tm_vertex(const o_trimesh *m, int i) { return V3(m->v[3 * i], m->v[3 * i + 1], m->v[3 * i + 2]); }
+
+/* VerticalHits (:96-121) folded into its two uses: mode 0 counts the hits above zq (Contains), mode 1 keeps the
+   highest (side 0) or lowest hit in *zext (SurfaceZ); returns the number of hits */
+static int tm_hits(const o_trimesh *m, double x, double y, int mode, double zq, int side, double *zext)
+{
+    int n = 0, above = 0;
+    if (x < m->mn[0] || x > m->mx[0] || y < m->mn[1] || y > m->mx[1]) return 0;
+    x += 1.2345e-7;
+    y += 2.3456e-7;
+    int cell = tm_cy2(m, y) * m->nx2 + tm_cx2(m, x);
+    for (int q = m->xy_start[cell]; q < m->xy_start[cell + 1]; q++) {
+        int t = m->xy_items[q];
+        v3 a = tm_vertex(m, m->t[3 * t]), b = tm_vertex(m, m->t[3 * t + 1]), c = tm_vertex(m, m->t[3 * t + 2]);
+        double d = (b.x - a.x) * (c.y - a.y) - (c.x - a.x) * (b.y - a.y);
+        if (fabs(d) < 1e-300) continue;
+        double u = ((x - a.x) * (c.y - a.y) - (c.x - a.x) * (y - a.y)) / d;
+        double v = ((b.x - a.x) * (y - a.y) - (x - a.x) * (b.y - a.y)) / d;
+        if (u < 0 || v < 0 || u + v > 1) continue;
+        double z = a.z + u * (b.z - a.z) + v * (c.z - a.z);
+        if (mode == 0) above += z > zq;
+        else *zext = n == 0 ? z : (side == 0 ? fmax(*zext, z) : fmin(*zext, z));
+        n++;
+    }
+    return mode == 0 ? above : n;
+}
+
+/* Contains (:125-137) */
+static int tm_contains(const o_trimesh *m, v3 p)
+{
+    if (p.x < m->mn[0] || p.x > m->mx[0] || p.y < m->mn[1] || p.y > m->mx[1] || p.z < m->mn[2] || p.z > m->mx[2]) return 0;
+    return (tm_hits(m, p.x, p.y, 0, p.z, 0, NULL) & 1) == 1;
+}
+
+/* Closest (:139-178) */
+static int tm_closest(const o_trimesh *m, v3 p, double maxd, v3 *point, v3 *normal, double *dist)
+{
+    *point = p;
+    *normal = V3(0, 0, 1);
+    int ci = (int)floor((p.x - m->mn[0]) / m->c3), cj = (int)floor((p.y - m->mn[1]) / m->c3), ck = (int)floor((p.z - m->mn[2]) / m->c3);
+    int max_ring = (int)ceil(maxd / m->c3) + 1;
+    double best = maxd * maxd;
+    for (int ring = 0; ring <= max_ring; ring++) {
+        for (int k = ck - ring; k <= ck + ring; k++) {
+            if (k < 0 || k >= m->gz) continue;
+            for (int j = cj - ring; j <= cj + ring; j++) {
+                if (j < 0 || j >= m->gy) continue;
+                int shell_row = abs(j - cj) == ring || abs(k - ck) == ring;
+                int istep = shell_row || ring == 0 ? 1 : 2 * ring;
+                for (int i = ci - ring; i <= ci + ring; i += istep) {
+                    if (i < 0 || i >= m->gx) continue;
+                    int cell = (k * m->gy + j) * m->gx + i;
+                    for (int q = m->g3_start[cell]; q < m->g3_start[cell + 1]; q++) {
+                        int t = m->g3_items[q];
+                        v3 a = tm_vertex(m, m->t[3 * t]), b = tm_vertex(m, m->t[3 * t + 1]), c = tm_vertex(m, m->t[3 * t + 2]);
+                        v3 cq = o_closest_on_triangle(p, a, b, c);
+                        double dd = vlen2(vsub(cq, p));
+                        if (dd >= best) continue;
+                        best = dd;
+                        *point = cq;
+                        *normal = vnormalized(vcross(vsub(b, a), vsub(c, a)));
+                    }
+                }
+            }
+        }
+        if (sqrt(best) <= ring * m->c3) break;
+    }
+    *dist = sqrt(best);
+    return *dist < maxd;
+}
+
+/* TriMeshDie.Clearance / Project / SurfaceZ (:267-296), Reach = 6 */
+static double tm_clearance(const o_trimesh *m, v3 p, double offset)
+{
+    const double reach = 6;
+    v3 q = V3(p.x, p.y, p.z - offset);
+    if (q.x < m->mn[0] - reach || q.x > m->mx[0] + reach || q.y < m->mn[1] - reach || q.y > m->mx[1] + reach ||
+        q.z < m->mn[2] - reach || q.z > m->mx[2] + reach)
+        return reach;
+    int inside = tm_contains(m, q);
+    v3 c, n;
+    double dist;
+    double d = tm_closest(m, q, reach, &c, &n, &dist) ? dist : reach;
+    return inside ? -d : d;
+}
+static v3 tm_project(const o_trimesh *m, int side, v3 p, double offset, v3 *normal)
+{
+    const double reach = 6;
+    v3 q = V3(p.x, p.y, p.z - offset), c, n;
+    double dist;
+    if (!tm_closest(m, q, 4 * reach, &c, &n, &dist)) n = side == 0 ? V3(0, 0, 1) : V3(0, 0, -1);
+    *normal = n;
+    return V3(c.x, c.y, c.z + offset);
+}
+static double tm_surface_z(const o_trimesh *m, int side, double x, double y)
+{
+    double z = 0;
+    return tm_hits(m, x, y, 1, 0, side, &z) ? z : NAN;
+}
+
 double hf_height(const o_hfdie *d, double x, double y)
 {
+    if (d->kind == 1) return tm_surface_z(&d->tm, d->side, x, y);
     double fx = dclamp((x - d->x0) / d->dx, 0, d->nx), fy = dclamp((y - d->y0) / d->dx, 0, d->ny);
     int i = imin((int)fx, d->nx - 1), j = imin((int)fy, d->ny - 1);
     double u = fx - i, v = fy - j;
@@ -81,6 +259,7 @@ double hf_height(const o_hfdie *d, double x, double y)
 /* ThreeD/HeightFieldDie.cs:130-134 */
 double hf_clearance(const o_hfdie *d, v3 p, double offset)
 {
+    if (d->kind == 1) return tm_clearance(&d->tm, p, offset);
     double h = hf_height(d, p.x, p.y) + offset;
     return d->side == 0 ? p.z - h : h - p.z;
 }
@@ -93,6 +272,7 @@ static v3 hf_vertex(const o_hfdie *d, int i, int j, double offset)
 /* ThreeD/HeightFieldDie.cs:157-191 */
 v3 hf_project(const o_hfdie *d, v3 p, double offset, v3 *normal)
 {
+    if (d->kind == 1) return tm_project(&d->tm, d->side, p, offset, normal);
     double reach = fabs(hf_clearance(d, p, offset)) + 1.5 * d->dx;
     int i0 = iclamp((int)floor((p.x - reach - d->x0) / d->dx), 0, d->nx - 1);
     int i1 = iclamp((int)floor((p.x + reach - d->x0) / d->dx), 0, d->nx - 1);

@@ -119,6 +119,8 @@ void o3d_destroy(o3d *s)
     free_mesh(s);
     free(s->die[0].h);
     free(s->die[1].h);
+    o_trimesh_free(&s->die[0].tm);
+    o_trimesh_free(&s->die[1].tm);
     ospd_destroy(s->lin);
     free(s);
 }
@@ -340,12 +342,32 @@ int o3d_set_die(o3d *s, int side, int nx, int ny, double x0, double y0, double d
     if (side < 0 || side > 1 || nx < 1 || ny < 1 || !(dx > 0)) return fail(s, E_INPUT, "invalid die");
     o_hfdie *d = &s->die[side];
     free(d->h);
+    o_trimesh_free(&d->tm);
+    d->kind = 0;
     d->side = side; d->nx = nx; d->ny = ny; d->x0 = x0; d->y0 = y0; d->dx = dx;
     d->h = NEW(double, (nx + 1) * (ny + 1));
     memcpy(d->h, h, sizeof(double) * (nx + 1) * (ny + 1));
     s->have_dies |= 1 << side;
     return E_OK;
 }
+
+/* TriMeshDie (ThreeD/TriMeshSolid.cs:248-297) in place of a height field */
+int o3d_set_trimesh_die(o3d *s, int side, int nv, const double *v, int nt, const int *tri)
+{
+    if (side < 0 || side > 1) return fail(s, E_INPUT, "invalid die");
+    o_hfdie *d = &s->die[side];
+    free(d->h);
+    d->h = NULL;
+    if (o_trimesh_build(&d->tm, nv, v, nt, tri) != 0) return fail(s, E_INPUT, "invalid triangulated die");
+    d->kind = 1;
+    d->side = side;
+    d->nx = d->ny = 1;
+    d->x0 = d->tm.mn[0]; d->y0 = d->tm.mn[1]; d->dx = d->tm.c2;
+    s->have_dies |= 1 << side;
+    return E_OK;
+}
+
+double o3d_die_height(o3d *s, int side, double x, double y) { return hf_height(&s->die[side], x, y); }
 
 double o3d_die_project(o3d *s, int side, const double *p, double offset, double *q, double *nrm)
 {

@@ -42,8 +42,24 @@ v3 o_closest_on_triangle(v3 p, v3 a, v3 b, v3 c);
 double o_tet_volume(v3 a, v3 b, v3 c, v3 d);
 double o_tet_quality4(v3 a, v3 b, v3 c, v3 d);
 
-/* Height-field die (ThreeD/HeightFieldDie.cs). */
-typedef struct { int side; double x0, y0, dx; int nx, ny; double *h; } o_hfdie;
+/* Triangulated solid (ThreeD/TriMeshSolid.cs:5-180): vertices, triangles, bounding box and its two bucket grids. */
+typedef struct {
+    int nv, nt;
+    double *v;
+    int *t;
+    double mn[3], mx[3];
+    double c2;
+    int nx2, ny2;
+    int *xy_start, *xy_items;
+    double c3;
+    int gx, gy, gz;
+    int *g3_start, *g3_items;
+} o_trimesh;
+int o_trimesh_build(o_trimesh *m, int nv, const double *v, int nt, const int *tri);
+void o_trimesh_free(o_trimesh *m);
+
+/* Die (ThreeD/HeightFieldDie.cs; kind 1: TriMeshDie, ThreeD/TriMeshSolid.cs:248-297). */
+typedef struct { int side; double x0, y0, dx; int nx, ny; double *h; int kind; o_trimesh tm; } o_hfdie;
 double hf_height(const o_hfdie *d, double x, double y);
 double hf_clearance(const o_hfdie *d, v3 p, double offset);
 v3 hf_project(const o_hfdie *d, v3 p, double offset, v3 *normal);

@@ -62,6 +62,8 @@ def _declare(L):
         "o3d_scalar": (C.c_double, [vp, C.c_char_p]), "o3d_set_scalar": (C.c_int, [vp, C.c_char_p, C.c_double]),
         "o3d_die_project": (C.c_double, [vp, C.c_int, dp, C.c_double, dp, dp]),
         "o3d_die_clearance": (C.c_double, [vp, C.c_int, dp, C.c_double]),
+        "o3d_set_trimesh_die": (C.c_int, [vp, C.c_int, C.c_int, dp, C.c_int, i32p]),
+        "o3d_die_height": (C.c_double, [vp, C.c_int, C.c_double, C.c_double]),
         "o3d_tet_quality": (C.c_double, [dp, dp, dp, dp]),
         "o3d_set_remesher": (None, [vp, REMESH_FN, vp]),
         "o3d_replace_mesh": (C.c_int, [vp, C.c_int, C.c_int, dp, i32p, u8p, u8p, u8p, dp, dp, dp, dp, dp, dp]),
@@ -129,8 +131,13 @@ class Oracle3D:
         self._check(L.o3d_set_mesh(self.h, len(x), len(t), _dp(x), t.ctypes.data_as(C.POINTER(C.c_int32)),
                                    ox.ctypes.data_as(C.POINTER(C.c_uint8)), oy.ctypes.data_as(C.POINTER(C.c_uint8))))
         for side, d in enumerate(dies):
-            hh = np.ascontiguousarray(d.h, np.float64)
-            self._check(L.o3d_set_die(self.h, side, d.nx, d.ny, d.x0, d.y0, d.dx, _dp(hh)))
+            if hasattr(d, "triangles"):
+                v = np.ascontiguousarray(d.vertices, np.float64)
+                tr = np.ascontiguousarray(d.triangles, np.int32)
+                self._check(L.o3d_set_trimesh_die(self.h, side, len(v), _dp(v), len(tr), tr.ctypes.data_as(C.POINTER(C.c_int32))))
+            else:
+                hh = np.ascontiguousarray(d.h, np.float64)
+                self._check(L.o3d_set_die(self.h, side, d.nx, d.ny, d.x0, d.y0, d.dx, _dp(hh)))
         self._check(L.o3d_init(self.h, mesh.gap0, *mesh.bounds_for_velocity))
 
     def _check(self, rc):
@@ -205,6 +212,8 @@ class Oracle3D:
 
         G = _lib.lib()
         vol_target = self.scalar("vol0") / self.p.sym_factor
+        if any(hasattr(d, "triangles") for d in dies):
+            raise NotImplementedError("the oracle remeshes with height-field dies only")
         self._die_keep = [np.ascontiguousarray(d.h, np.float64) for d in dies]
         grids = [_lib.DieGrid(d.nx, d.ny, d.x0, d.y0, d.dx, hh.ctypes.data_as(C.POINTER(C.c_double)))
                  for d, hh in zip(dies, self._die_keep)]
@@ -252,6 +261,9 @@ class Oracle3D:
     def die_clearance(self, side, p, offset):
         p = np.ascontiguousarray(p, np.float64)
         return self.L.o3d_die_clearance(self.h, side, _dp(p), offset)
+
+    def die_height(self, side, x, y):
+        return self.L.o3d_die_height(self.h, side, float(x), float(y))
 
 
 class OracleSpd:
