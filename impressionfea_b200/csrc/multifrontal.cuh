@@ -41,9 +41,12 @@ struct Dev {
     T *F, *U, *Inv, *Xinv, *Abig;
 };
 
-// Fronts at least this tall get a full pivot-block inverse and multi-CTA solves; shorter ones are eliminated by
-// one CTA each.
+// Fronts at least this tall (and with more than kWideMinCols pivot columns) get a full pivot-block inverse and
+// multi-CTA solves; the others are eliminated by one CTA each. Sending the narrow tall fronts (two panels or less)
+// to the one-CTA path as well measured slower on the closed-die factor (1.77 against 1.46 ms per solve), so the
+// column bound is off.
 constexpr int kWideM = 192;
+constexpr int kWideMinCols = 0;
 
 // Rows (or columns) of a 64-wide tile owned by thread index t (0..15): four consecutive ones in single precision
 // (one 16-byte shared-memory load), pairs {2t, 2t + 1} and {2t + 32, 2t + 33} in double precision (two 16-byte
@@ -1435,7 +1438,7 @@ public:
             big_start_[l] = (int32_t)big_list_.size();
             for (int32_t q = S.level_start[l]; q < S.level_start[l + 1]; q++) {
                 int sn = S.level_list[q];
-                if (S.m[sn] >= wide_m_) {
+                if (S.m[sn] >= wide_m_ && S.ncol[sn] > mf::kWideMinCols) {
                     big_list_.push_back(sn);
                     xinv_off_[sn] = xinv_total;
                     xinv_total += (int64_t)S.ncol[sn] * S.ncol[sn];

@@ -1419,7 +1419,7 @@ struct Forging3D {
         A("contact", d_contact, nn) A("release", d_release, nn) A("fixed", d_fixed, nd) A("n_fix", d_nfix, nn)
         A("die_axis", d_dieaxis, nn) A("nbr_start", d_nbr_start, nn + 1) A("nbr", d_nbr, topo.nbr.size())
         A("e_r", d_er, 12 * ne) A("g_coef", d_gcoef, 3 * topo.g_node.size()) A("g_node", d_gnode, topo.g_node.size())
-        A("g_start", d_gstart, nn + 1) A("vg_prev", d_vgprev, 3 * nn)
+        A("g_start", d_gstart, nn + 1) A("vg_prev", d_vgprev, 3 * nn) A("tets", d_tets, 4 * ne)
 #undef A
         if (nm == "e_nbr") return ArrRef{(void *)topo.e_nbr.data(), topo.e_nbr.size(), -4};
         if (nm == "bface") return ArrRef{(void *)topo.bface.data(), topo.bface.size(), -4};
