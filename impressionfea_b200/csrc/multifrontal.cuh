@@ -623,15 +623,14 @@ template <typename T>
 static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32_t *__restrict__ fronts, T *y, T *Y1)
 {
     const int s = fronts[blockIdx.y];
-    const int nc = D.ncol[s], c0 = D.c0[s], lane = threadIdx.x & 31;
-    // warp w of CTA b takes rows nc - 1 - (16 b + w), then every 16 gridDim.x-th row further up
-    for (int q = blockIdx.x * 16 + (threadIdx.x >> 5); q < nc; q += gridDim.x * 16) {
-        const int r = nc - 1 - q;
-        const T v = warp_dot(D.Xinv + D.xinv_off[s] + (int64_t)r * nc, D.Abig + D.idx_start[s], r + 1, lane);
-        if (lane == 0) {
-            y[c0 + r] = v;
-            Y1[D.idx_start[s] + r] = v;
-        }
+    const int nc = D.ncol[s], c0 = D.c0[s], ntile = (nc + 15) / 16;
+    if ((int)blockIdx.x >= ntile) return;
+    const int r = (ntile - 1 - blockIdx.x) * 16 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (r >= nc) return;
+    const T v = warp_dot(D.Xinv + D.xinv_off[s] + (int64_t)r * nc, D.Abig + D.idx_start[s], r + 1, lane);
+    if (lane == 0) {
+        y[c0 + r] = v;
+        Y1[D.idx_start[s] + r] = v;
     }
 }
 
@@ -640,29 +639,29 @@ template <typename T>
 static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32_t *__restrict__ fronts, const T *Y1)
 {
     const int s = fronts[blockIdx.y];
-    const int ms = D.m[s], nc = D.ncol[s], nr = ms - nc, lane = threadIdx.x & 31;
-    for (int i = blockIdx.x * 16 + (threadIdx.x >> 5); i < nr; i += gridDim.x * 16) {
-        const T v = warp_dot(D.F + D.front_off[s] + (int64_t)(nc + i) * ms, Y1 + D.idx_start[s], nc, lane);
-        if (lane == 0) D.U[D.uvec_start[s] + i] = -D.Abig[D.idx_start[s] + nc + i] + v;
-    }
+    const int ms = D.m[s], nc = D.ncol[s], nr = ms - nc;
+    const int i = blockIdx.x * 16 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= nr) return;
+    const T v = warp_dot(D.F + D.front_off[s] + (int64_t)(nc + i) * ms, Y1 + D.idx_start[s], nc, lane);
+    if (lane == 0) D.U[D.uvec_start[s] + i] = -D.Abig[D.idx_start[s] + nc + i] + v;
 }
 
 // z = y1 - L21^T x2, one warp per pivot column; x2 is read through the front's row indices as the column
 // streams (the CTA's warps read the same entries, from L1), sixteen column loads in flight per lane.
 template <typename T>
-__device__ __forceinline__ void dev_wide_bwd_z(Dev<T> D, int s, int tile, int ntz, const T *x, T *Z)
+__device__ __forceinline__ void dev_wide_bwd_z(Dev<T> D, int s, int tile, const T *x, T *Z)
 {
-    int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s], nr = ms - nc, lane = threadIdx.x & 31;
+    int ms = D.m[s], nc = D.ncol[s], c0 = D.c0[s], nr = ms - nc;
+    int k = tile * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (k >= nc) return;
     const int32_t *__restrict__ ix = D.idx + D.idx_start[s] + nc;
-    // ntz CTAs share the front's columns: warp w of CTA `tile` takes column 16 tile + w, then every 16 ntz-th
-    for (int k = tile * (blockDim.x >> 5) + (threadIdx.x >> 5); k < nc; k += ntz * (blockDim.x >> 5)) {
-        const T *__restrict__ col = D.F + D.front_off[s] + (int64_t)k * ms + nc;
-        T v = 0;
+    const T *__restrict__ col = D.F + D.front_off[s] + (int64_t)k * ms + nc;
+    int lane = threadIdx.x & 31;
+    T v = 0;
 #pragma unroll 16
-        for (int i = lane; i < nr; i += 32) v = fma(col[i], __ldg(x + __ldg(ix + i)), v);
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) Z[D.idx_start[s] + k] = x[c0 + k] - v;
-    }
+    for (int i = lane; i < nr; i += 32) v = fma(col[i], __ldg(x + __ldg(ix + i)), v);
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) Z[D.idx_start[s] + k] = x[c0 + k] - v;
 }
 
 // x1 = X^T z, one warp per pivot column j (column j of X is contiguous); z is staged in shared memory. Column
@@ -670,17 +669,24 @@ __device__ __forceinline__ void dev_wide_bwd_z(Dev<T> D, int s, int tile, int nt
 template <typename T>
 __device__ __forceinline__ void dev_wide_bwd_x(Dev<T> D, int s, int tile, const T *Z, T *x)
 {
-    const int nc = D.ncol[s], c0 = D.c0[s], lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    extern __shared__ __align__(16) unsigned char zs_raw[];
+    T *zs = (T *)zs_raw;
+    int nc = D.ncol[s], c0 = D.c0[s];
+    int nw = blockDim.x >> 5, nblk = (nc + nw - 1) / nw;
+    if (tile >= nblk) return;
+    int jbase = (nblk - 1 - tile) * nw;
     const T *z = Z + D.idx_start[s];
-    // warp w of CTA `tile` takes column 16 tile + w counted from the left (the longest), then every 16 gridDim.x-th
-    for (int j = tile * nw + (threadIdx.x >> 5); j < nc; j += gridDim.x * nw) {
-        const T *col = D.Xinv + D.xinv_off[s] + (int64_t)j * nc;
-        T v = 0;
-#pragma unroll 16
-        for (int i = j + lane; i < nc; i += 32) v = fma(col[i], __ldg(z + i), v);
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) x[c0 + j] = v;
-    }
+    for (int i = jbase + threadIdx.x; i < nc; i += blockDim.x) zs[i - jbase] = z[i];
+    __syncthreads();
+    int j = jbase + (threadIdx.x >> 5);
+    if (j >= nc) return;
+    const T *col = D.Xinv + D.xinv_off[s] + (int64_t)j * nc;
+    int lane = threadIdx.x & 31;
+    T v = 0;
+#pragma unroll 8
+    for (int i = j + lane; i < nc; i += 32) v = fma(col[i], zs[i - jbase], v);
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) x[c0 + j] = v;
 }
 template <typename T>
 static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev<T> D, const int32_t *__restrict__ fronts, const T *Z, T *x)
@@ -1216,7 +1222,7 @@ static __global__ void __launch_bounds__(512) k_bwd_level(Dev<T> D, const int32_
         dev_backward(D, small[blockIdx.x], x, x);
     } else {
         int t = blockIdx.x - nsmall;
-        dev_wide_bwd_z(D, big[t / ntz], t % ntz, ntz, x, Z);
+        dev_wide_bwd_z(D, big[t / ntz], t % ntz, x, Z);
     }
 }
 
@@ -1457,6 +1463,10 @@ public:
             mirror_tiles_ = ts.back();
             d_mirror_ts_.upload(ts, st_);
         }
+        wide_smem_ = 8;
+        for (int sn : big_list_) wide_smem_ = std::max(wide_smem_, (size_t)std::max(S.ncol[sn], S.m[sn] - S.ncol[sn]) * sizeof(T));
+        if (wide_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the wide solve kernels' shared-memory window");
+        ensure_dynamic_smem((const void *)mf::k_wide_bwd_x<T>, (int)wide_smem_);
         // inverse passes of the wide supernodes, per level: diagonal copies, then for groups of 2, 4, ... blocks
         // the T pass and the X21 pass, each followed by its reduction when a block range was split
         std::vector<mf::XTask> tasks;
@@ -1829,21 +1839,19 @@ public:
                     mnc = std::max(mnc, S.ncol[big_list_[q]]);
                     mnr = std::max(mnr, S.m[big_list_[q]] - S.ncol[big_list_[q]]);
                 }
-                // about four 512-thread CTAs per SM over the level's fronts; each warp takes several rows
-                int cap = std::max(1, (4 * 148 + bc - 1) / bc);
-                mf::k_wide_fwd_y<T><<<dim3(std::min((mnc + 15) / 16, cap), bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
-                mf::k_wide_fwd_t<T><<<dim3(std::min((mnr + 15) / 16, cap), bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
+                mf::k_wide_fwd_y<T><<<dim3((mnc + 15) / 16, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
+                mf::k_wide_fwd_t<T><<<dim3((mnr + 15) / 16, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
             }
         }
         for (int l = S.nlevels - 1; l >= 0; l--) {
             int q0 = small_start_[l], cnt = small_start_[l + 1] - q0;
             int b0 = big_start_[l], bc = big_start_[l + 1] - b0;
-            int ntz = bc > 0 ? std::min((S.ncol[big_list_[b0]] + 15) / 16, std::max(1, (4 * 148 + bc - 1) / bc)) : 1;
+            int ntz = bc > 0 ? (S.ncol[big_list_[b0]] + 15) / 16 : 1;
             if (cnt + bc > 0)
                 mf::k_bwd_level<T><<<cnt + bc * ntz, 512, level_smem_, st>>>(dev_, d_small_.p + q0, cnt, d_big_.p + b0, ntz,
                                                                             d_y_, d_z_);
             if (bc > 0)
-                mf::k_wide_bwd_x<T><<<dim3(ntz, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
+                mf::k_wide_bwd_x<T><<<dim3(ntz, bc), 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
         }
     }
 
@@ -1896,7 +1904,7 @@ private:
     DBuf<mf::XTask> d_xinv_tasks_;
     DBuf<T> d_xinv_w_;
     static constexpr int kXinvChunk = 4;  // tile steps per CTA before a block range is split
-    size_t small_smem_ = 8, level_smem_ = 8;
+    size_t small_smem_ = 8, wide_smem_ = 8, level_smem_ = 8;
     DBuf<int64_t> d_inv_off_, d_xinv_off_;
     DBuf<int64_t> d_mirror_ts_;   // the wide fronts' mirror tiles, prefix per front
     int64_t mirror_tiles_ = 0;
