@@ -530,6 +530,31 @@ static __global__ void k_xinv_reduce(Dev<T> D, const XTask *__restrict__ tasks, 
 // ---------------------------------------------------------------- solves of wide supernodes (batched multi-CTA GEMVs)
 // Per-front scratch vectors live at offset idx_start[s] (length m) in Abig (assembled right-hand side), Y1, Z.
 
+template <typename T>
+constexpr int kDotU = sizeof(T) == 4 ? 16 : 8;  // factor loads in flight per lane in the wide-front GEMVs
+
+// acc + sum of fa(c) fb(c) over c = first, first + G, .. < len (one lane's share of a dot product over G lanes). The
+// operands are loaded U at a time before any is used, so a lane keeps U loads in flight however short the run
+// (a plain strided loop waits out one memory latency per G elements); the products are added in the same order
+// as that loop's, so the sum is the same.
+template <int U, int G = 32, typename T, typename FA, typename FB>
+__device__ __forceinline__ T lane_dot(int first, int len, FA fa, FB fb, T acc)
+{
+    for (int c0 = first; c0 < len; c0 += G * U) {
+        T a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int c = c0 + G * u;
+            a[u] = c < len ? fa(c) : T(0);
+            b[u] = c < len ? fb(c) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (c0 + G * u < len) acc = fma(a[u], b[u], acc);
+    }
+    return acc;
+}
+
 // acc = [b(cols); 0] - children's update vectors (in child order).
 template <typename T>
 __device__ __forceinline__ void dev_wide_acc(Dev<T> D, int s, const T *y, int chunk, int nchunk)
@@ -605,49 +630,60 @@ static __global__ void __launch_bounds__(256) k_mirror(Dev<T> D, const int32_t *
     }
 }
 
-// One row of a mirrored operand against a vector: warp-wide dot product over a contiguous run, sixteen loads in
-// flight per lane, lanes summed by a shuffle tree (fixed order).
-template <typename T>
-__device__ __forceinline__ T warp_dot(const T *__restrict__ row, const T *__restrict__ v, int len, int lane)
+// One row of a mirrored operand against a vector: a dot product over a contiguous run by a group of G lanes
+// (G = 32: the whole warp; 16 or 8 for short rows, several rows to a warp), kDotU loads of each operand in flight
+// per lane, the group's lanes summed by a shuffle tree (fixed order). Every lane of the warp takes part in the
+// shuffles; a lane whose row does not exist passes len = 0.
+template <int G, typename T>
+__device__ __forceinline__ T group_dot(const T *__restrict__ row, const T *__restrict__ v, int len, int gl)
 {
-    T acc = 0;
-#pragma unroll 16
-    for (int c = lane; c < len; c += 32) acc = fma(row[c], __ldg(v + c), acc);
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    T acc = lane_dot<kDotU<T>, G>(gl, len, [&](int c) { return row[c]; }, [&](int c) { return __ldg(v + c); }, T(0));
+    for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     return acc;
 }
 
-// y1 = X acc1 (X lower triangular, read through its mirror: row r is X(c, r) for c <= r, contiguous), one warp
-// per row, 16 rows per CTA counted from the bottom (longest rows first)
-template <typename T>
+// Lanes per row of the forward GEMVs of a level whose longest row has `len` entries.
+inline int fwd_group(int len) { return len <= 96 ? 8 : len <= 224 ? 16 : 32; }
+
+// y1 = X acc1 (X lower triangular, read through its mirror: row r is X(c, r) for c <= r, contiguous), G lanes
+// per row, 16 * 32 / G rows per CTA counted from the bottom (longest rows first)
+template <typename T, int G>
 static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32_t *__restrict__ fronts, T *y, T *Y1)
 {
+    constexpr int RPC = 16 * (32 / G);
     const int s = fronts[blockIdx.y];
-    const int nc = D.ncol[s], c0 = D.c0[s], ntile = (nc + 15) / 16;
+    const int nc = D.ncol[s], c0 = D.c0[s], ntile = (nc + RPC - 1) / RPC;
     if ((int)blockIdx.x >= ntile) return;
-    const int r = (ntile - 1 - blockIdx.x) * 16 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (r >= nc) return;
-    const T v = warp_dot(D.Xinv + D.xinv_off[s] + (int64_t)r * nc, D.Abig + D.idx_start[s], r + 1, lane);
-    if (lane == 0) {
+    const int lane = threadIdx.x & 31;
+    const int r = (ntile - 1 - blockIdx.x) * RPC + (threadIdx.x >> 5) * (32 / G) + lane / G;
+    if ((threadIdx.x >> 5) * (32 / G) + (ntile - 1 - blockIdx.x) * RPC >= nc) return;  // the warp's first row
+    const bool ok = r < nc;
+    const T v = group_dot<G>(D.Xinv + D.xinv_off[s] + (int64_t)(ok ? r : 0) * nc, D.Abig + D.idx_start[s],
+                             ok ? r + 1 : 0, lane % G);
+    if (ok && lane % G == 0) {
         y[c0 + r] = v;
         Y1[D.idx_start[s] + r] = v;
     }
 }
 
-// update vector t = -acc2 + L21 y1 (L21 through its mirror: row i is F(k, nc + i), k < nc), one warp per row
-template <typename T>
+// update vector t = -acc2 + L21 y1 (L21 through its mirror: row i is F(k, nc + i), k < nc), G lanes per row
+template <typename T, int G>
 static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32_t *__restrict__ fronts, const T *Y1)
 {
+    constexpr int RPC = 16 * (32 / G);
     const int s = fronts[blockIdx.y];
     const int ms = D.m[s], nc = D.ncol[s], nr = ms - nc;
-    const int i = blockIdx.x * 16 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (i >= nr) return;
-    const T v = warp_dot(D.F + D.front_off[s] + (int64_t)(nc + i) * ms, Y1 + D.idx_start[s], nc, lane);
-    if (lane == 0) D.U[D.uvec_start[s] + i] = -D.Abig[D.idx_start[s] + nc + i] + v;
+    const int lane = threadIdx.x & 31, w0 = blockIdx.x * RPC + (threadIdx.x >> 5) * (32 / G);
+    if (w0 >= nr) return;  // the warp's first row
+    const int i = w0 + lane / G;
+    const bool ok = i < nr;
+    const T v = group_dot<G>(D.F + D.front_off[s] + (int64_t)(nc + (ok ? i : 0)) * ms, Y1 + D.idx_start[s],
+                             ok ? nc : 0, lane % G);
+    if (ok && lane % G == 0) D.U[D.uvec_start[s] + i] = -D.Abig[D.idx_start[s] + nc + i] + v;
 }
 
 // z = y1 - L21^T x2, one warp per pivot column; x2 is read through the front's row indices as the column
-// streams (the CTA's warps read the same entries, from L1), sixteen column loads in flight per lane.
+// streams (the CTA's warps read the same entries, from L1), kDotU column loads in flight per lane.
 template <typename T>
 __device__ __forceinline__ void dev_wide_bwd_z(Dev<T> D, int s, int tile, const T *x, T *Z)
 {
@@ -657,9 +693,8 @@ __device__ __forceinline__ void dev_wide_bwd_z(Dev<T> D, int s, int tile, const 
     const int32_t *__restrict__ ix = D.idx + D.idx_start[s] + nc;
     const T *__restrict__ col = D.F + D.front_off[s] + (int64_t)k * ms + nc;
     int lane = threadIdx.x & 31;
-    T v = 0;
-#pragma unroll 16
-    for (int i = lane; i < nr; i += 32) v = fma(col[i], __ldg(x + __ldg(ix + i)), v);
+    T v = lane_dot<kDotU<T>>(lane, nr, [&](int i) { return col[i]; }, [&](int i) { return __ldg(x + __ldg(ix + i)); },
+                             T(0));
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) Z[D.idx_start[s] + k] = x[c0 + k] - v;
 }
@@ -682,9 +717,7 @@ __device__ __forceinline__ void dev_wide_bwd_x(Dev<T> D, int s, int tile, const 
     if (j >= nc) return;
     const T *col = D.Xinv + D.xinv_off[s] + (int64_t)j * nc;
     int lane = threadIdx.x & 31;
-    T v = 0;
-#pragma unroll 8
-    for (int i = j + lane; i < nc; i += 32) v = fma(col[i], zs[i - jbase], v);
+    T v = lane_dot<8>(j + lane, nc, [&](int i) { return col[i]; }, [&](int i) { return zs[i - jbase]; }, T(0));
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) x[c0 + j] = v;
 }
@@ -1128,8 +1161,8 @@ __device__ __forceinline__ void dev_forward(Dev<T> D, int s, T *y)
         const T *I = Inv + (int64_t)(kb / PW) * PW * PW;
         // y_blk = Linv acc_blk (warp per output row, coalesced over the inverse's columns? rows: I[c*PW + i])
         for (int i = warp; i < w; i += nw) {
-            T v = 0;
-            for (int c = lane; c <= i; c += 32) v = fma(I[(int64_t)c * PW + i], acc[kb + c], v);
+            T v = lane_dot<2>(lane, i + 1, [&](int c) { return I[(int64_t)c * PW + i]; }, [&](int c) { return acc[kb + c]; },
+                              T(0));
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) yb[i] = v;
         }
@@ -1138,8 +1171,15 @@ __device__ __forceinline__ void dev_forward(Dev<T> D, int s, T *y)
         // rows below the block
         for (int r = kb + w + tid; r < ms; r += nt) {
             T v = acc[r];
-#pragma unroll 8
-            for (int k = 0; k < w; k++) v = fma(-F[(int64_t)(kb + k) * ms + r], yb[k], v);
+            // the block's w <= 64 entries of row r, 16 loads in flight
+            for (int k0 = 0; k0 < w; k0 += 16) {
+                T f[16];
+#pragma unroll
+                for (int u = 0; u < 16; u++) f[u] = k0 + u < w ? F[(int64_t)(kb + k0 + u) * ms + r] : T(0);
+#pragma unroll
+                for (int u = 0; u < 16; u++)
+                    if (k0 + u < w) v = fma(-f[u], yb[k0 + u], v);
+            }
             acc[r] = v;
         }
         __syncthreads();
@@ -1167,8 +1207,7 @@ __device__ __forceinline__ void dev_backward(Dev<T> D, int s, const T *y, T *x)
     __syncthreads();
     for (int k = warp; k < nc; k += nw) {
         const T *col = F + (int64_t)k * ms + nc;
-        T v = 0;
-        for (int i = lane; i < nr; i += 32) v = fma(col[i], xs[i], v);
+        T v = lane_dot<8>(lane, nr, [&](int i) { return col[i]; }, [&](int i) { return xs[i]; }, T(0));
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
         if (lane == 0) acc[k] -= v;
     }
@@ -1178,8 +1217,7 @@ __device__ __forceinline__ void dev_backward(Dev<T> D, int s, const T *y, T *x)
         int kb = bi * PW, w = min(PW, nc - kb), ke = kb + w;
         for (int j = kb + warp; j < ke; j += nw) {
             const T *col = F + (int64_t)j * ms;
-            T v = 0;
-            for (int k = ke + lane; k < nc; k += 32) v = fma(col[k], acc[k], v);
+            T v = lane_dot<8>(ke + lane, nc, [&](int k) { return col[k]; }, [&](int k) { return acc[k]; }, T(0));
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) acc[j] -= v;
         }
@@ -1187,8 +1225,8 @@ __device__ __forceinline__ void dev_backward(Dev<T> D, int s, const T *y, T *x)
         // x_blk = Linv^T acc_blk: x_j = sum_{i >= j} Linv[i][j] acc_i (column j of the inverse is contiguous)
         const T *I = Inv + (int64_t)bi * PW * PW;
         for (int j = warp; j < w; j += nw) {
-            T v = 0;
-            for (int i = j + lane; i < w; i += 32) v = fma(I[(int64_t)j * PW + i], acc[kb + i], v);
+            T v = lane_dot<2>(j + lane, w, [&](int i) { return I[(int64_t)j * PW + i]; }, [&](int i) { return acc[kb + i]; },
+                              T(0));
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) xb[j] = v;
         }
@@ -1839,8 +1877,19 @@ public:
                     mnc = std::max(mnc, S.ncol[big_list_[q]]);
                     mnr = std::max(mnr, S.m[big_list_[q]] - S.ncol[big_list_[q]]);
                 }
-                mf::k_wide_fwd_y<T><<<dim3((mnc + 15) / 16, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
-                mf::k_wide_fwd_t<T><<<dim3((mnr + 15) / 16, bc), 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
+                // short rows (the lower levels' pivot counts) share a warp: G lanes per row, 16 * 32 / G rows per CTA
+                const int g = mf::fwd_group(mnc), rpc = 16 * (32 / g);
+                const dim3 gy((mnc + rpc - 1) / rpc, bc), gt((mnr + rpc - 1) / rpc, bc);
+                if (g == 8) {
+                    mf::k_wide_fwd_y<T, 8><<<gy, 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
+                    mf::k_wide_fwd_t<T, 8><<<gt, 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
+                } else if (g == 16) {
+                    mf::k_wide_fwd_y<T, 16><<<gy, 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
+                    mf::k_wide_fwd_t<T, 16><<<gt, 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
+                } else {
+                    mf::k_wide_fwd_y<T, 32><<<gy, 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
+                    mf::k_wide_fwd_t<T, 32><<<gt, 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
+                }
             }
         }
         for (int l = S.nlevels - 1; l >= 0; l--) {
