@@ -1,6 +1,8 @@
 // multifrontal.cpp — symbolic analysis of the GPU multifrontal Cholesky (see multifrontal.h).
 #include "multifrontal.h"
 
+#include "host_par.h"
+
 #include <cusolverSp.h>
 #include <cusparse.h>
 
@@ -274,20 +276,28 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
     if (block < 1 || n % block) block = 1;
     const int nb = n / block;
 
-    // 1. nested dissection of the block graph (no self loops)
+    // 1. nested dissection of the block graph (no self loops); per chunk of nodes, joined in node order
     std::vector<int> gp(nb + 1, 0), gi;
     {
-        std::vector<int> mark(nb, -1);
-        for (int b = 0; b < nb; b++) {
-            int d = b * block;
-            for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
-                int o = ri[p] / block;
-                if (o == b || mark[o] == b) continue;
-                mark[o] = b;
-                gi.push_back(o);
+        std::vector<std::vector<int>> part(par_chunk_count(nb));
+        par_chunks(nb, [&](int t, int b0, int b1) {
+            std::vector<int> mark(nb, -1);
+            part[t].reserve((size_t)(cp[(size_t)b1 * block] - cp[(size_t)b0 * block]) / (block * block));
+            for (int b = b0; b < b1; b++) {
+                int d = b * block, c = 0;
+                for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
+                    int o = ri[p] / block;
+                    if (o == b || mark[o] == b) continue;
+                    mark[o] = b;
+                    part[t].push_back(o);
+                    c++;
+                }
+                gp[b + 1] = c;
             }
-            gp[b + 1] = (int)gi.size();
-        }
+        });
+        for (int b = 0; b < nb; b++) gp[b + 1] += gp[b];
+        gi.reserve(gp[nb]);
+        for (auto &v : part) gi.insert(gi.end(), v.begin(), v.end());
     }
     std::vector<int> pnode(nb);
     if (!gi.empty() && node_xyz) {
@@ -311,40 +321,48 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
     //     row structures carry over node by node. Otherwise they run on the matrix itself.
     bool nodal = block > 1, sorted_rows = true;
     if (nodal) {
-        std::vector<int> rmark(n, -1), dmark(n, -1);
-        for (int b = 0; b < nb && nodal; b++) {
-            // rows of node b's blocks: its own and its neighbours'
-            for (int c = 0; c < block; c++) rmark[b * block + c] = b;
-            for (int p = gp[b]; p < gp[b + 1]; p++)
-                for (int c = 0; c < block; c++) rmark[gi[p] * block + c] = b;
-            int64_t want = (int64_t)block * (gp[b + 1] - gp[b] + 1);
-            for (int c = 0; c < block && nodal; c++) {
-                int d = b * block + c;
-                if (cp[d + 1] - cp[d] != want) {
-                    nodal = false;
-                    break;
-                }
-                // rows in range, in the node's blocks and all distinct (strictly increasing rows need no marks)
-                bool inc = true;
-                for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
-                    int r = ri[p];
-                    if ((unsigned)r >= (unsigned)n || rmark[r] != b) {
+        std::atomic<bool> all_nodal{true}, all_sorted{true};
+        par_chunks(nb, [&](int, int b0, int b1) {
+            bool nodal = true, sorted_rows = true;
+            std::vector<int> rmark(n, -1), dmark(n, -1);
+            for (int b = b0; b < b1 && nodal && all_nodal; b++) {
+                // rows of node b's blocks: its own and its neighbours'
+                for (int c = 0; c < block; c++) rmark[b * block + c] = b;
+                for (int p = gp[b]; p < gp[b + 1]; p++)
+                    for (int c = 0; c < block; c++) rmark[gi[p] * block + c] = b;
+                int64_t want = (int64_t)block * (gp[b + 1] - gp[b] + 1);
+                for (int c = 0; c < block && nodal; c++) {
+                    int d = b * block + c;
+                    if (cp[d + 1] - cp[d] != want) {
                         nodal = false;
                         break;
                     }
-                    if (p > cp[d] && r <= ri[p - 1]) inc = false;
-                }
-                sorted_rows = sorted_rows && inc;
-                if (nodal && !inc)
+                    // rows in range, in the node's blocks and all distinct (strictly increasing rows need no marks)
+                    bool inc = true;
                     for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
-                        if (dmark[ri[p]] == d) {
+                        int r = ri[p];
+                        if ((unsigned)r >= (unsigned)n || rmark[r] != b) {
                             nodal = false;
                             break;
                         }
-                        dmark[ri[p]] = d;
+                        if (p > cp[d] && r <= ri[p - 1]) inc = false;
                     }
+                    sorted_rows = sorted_rows && inc;
+                    if (nodal && !inc)
+                        for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
+                            if (dmark[ri[p]] == d) {
+                                nodal = false;
+                                break;
+                            }
+                            dmark[ri[p]] = d;
+                        }
+                }
             }
-        }
+            if (!nodal) all_nodal = false;
+            if (!sorted_rows) all_sorted = false;
+        });
+        nodal = all_nodal;
+        sorted_rows = all_sorted;
     }
     const int B = nodal ? block : 1, ns = n / B;  // structural granularity and column count
     const int32_t *scp = cp, *sri = ri;
@@ -724,7 +742,7 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
         for (int k = 0; k < m[s]; k++) pos[ib[k]] = -1;
         return cnt;
     };
-    int nth = cp[n] < (1 << 18) ? 1 : (int)std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+    int nth = cp[n] < (1 << 18) ? 1 : (int)std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
     nth = std::max(1, std::min(nth, nsuper));
     std::vector<std::vector<int32_t>> tpos(nth, std::vector<int32_t>(n, -1));
     auto each_front = [&](const std::function<void(int, std::vector<int32_t> &)> &body) {

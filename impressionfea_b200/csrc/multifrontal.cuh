@@ -699,32 +699,36 @@ __device__ __forceinline__ void dev_wide_bwd_z(Dev<T> D, int s, int tile, const 
     if (lane == 0) Z[D.idx_start[s] + k] = x[c0 + k] - v;
 }
 
-// x1 = X^T z, one warp per pivot column j (column j of X is contiguous); z is staged in shared memory. Column
-// group `tile` counted from the right end (leftmost, longest columns first).
-template <typename T>
+// x1 = X^T z, G lanes per pivot column j (column j of X is contiguous; G = 32 a warp, 16 or 8 for short columns,
+// several to a warp); z is staged in shared memory. Column group `tile` (16 * 32 / G columns) counted from the
+// right end (leftmost, longest columns first).
+template <typename T, int G>
 __device__ __forceinline__ void dev_wide_bwd_x(Dev<T> D, int s, int tile, const T *Z, T *x)
 {
     extern __shared__ __align__(16) unsigned char zs_raw[];
     T *zs = (T *)zs_raw;
+    constexpr int CPW = 32 / G;
     int nc = D.ncol[s], c0 = D.c0[s];
-    int nw = blockDim.x >> 5, nblk = (nc + nw - 1) / nw;
+    int cpc = (blockDim.x >> 5) * CPW, nblk = (nc + cpc - 1) / cpc;
     if (tile >= nblk) return;
-    int jbase = (nblk - 1 - tile) * nw;
+    int jbase = (nblk - 1 - tile) * cpc;
     const T *z = Z + D.idx_start[s];
     for (int i = jbase + threadIdx.x; i < nc; i += blockDim.x) zs[i - jbase] = z[i];
     __syncthreads();
-    int j = jbase + (threadIdx.x >> 5);
-    if (j >= nc) return;
-    const T *col = D.Xinv + D.xinv_off[s] + (int64_t)j * nc;
-    int lane = threadIdx.x & 31;
-    T v = lane_dot<8>(j + lane, nc, [&](int i) { return col[i]; }, [&](int i) { return zs[i - jbase]; }, T(0));
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) x[c0 + j] = v;
+    int lane = threadIdx.x & 31, jw = jbase + (threadIdx.x >> 5) * CPW;
+    if (jw >= nc) return;  // the warp's first column
+    int j = jw + lane / G;
+    const bool ok = j < nc;
+    const T *col = D.Xinv + D.xinv_off[s] + (int64_t)(ok ? j : 0) * nc;
+    T v = lane_dot<8, G>((ok ? j : nc) + lane % G, nc, [&](int i) { return col[i]; }, [&](int i) { return zs[i - jbase]; },
+                         T(0));
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (ok && lane % G == 0) x[c0 + j] = v;
 }
-template <typename T>
+template <typename T, int G>
 static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev<T> D, const int32_t *__restrict__ fronts, const T *Z, T *x)
 {
-    dev_wide_bwd_x(D, fronts[blockIdx.y], blockIdx.x, Z, x);
+    dev_wide_bwd_x<T, G>(D, fronts[blockIdx.y], blockIdx.x, Z, x);
 }
 
 // Trailing update of every listed front by its pivot columns [k0, k0 + kd), kd = min(kdepth, ncol - k0):
@@ -1504,7 +1508,9 @@ public:
         wide_smem_ = 8;
         for (int sn : big_list_) wide_smem_ = std::max(wide_smem_, (size_t)std::max(S.ncol[sn], S.m[sn] - S.ncol[sn]) * sizeof(T));
         if (wide_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the wide solve kernels' shared-memory window");
-        ensure_dynamic_smem((const void *)mf::k_wide_bwd_x<T>, (int)wide_smem_);
+        ensure_dynamic_smem((const void *)mf::k_wide_bwd_x<T, 8>, (int)wide_smem_);
+        ensure_dynamic_smem((const void *)mf::k_wide_bwd_x<T, 16>, (int)wide_smem_);
+        ensure_dynamic_smem((const void *)mf::k_wide_bwd_x<T, 32>, (int)wide_smem_);
         // inverse passes of the wide supernodes, per level: diagonal copies, then for groups of 2, 4, ... blocks
         // the T pass and the X21 pass, each followed by its reduction when a block range was split
         std::vector<mf::XTask> tasks;
@@ -1899,8 +1905,13 @@ public:
             if (cnt + bc > 0)
                 mf::k_bwd_level<T><<<cnt + bc * ntz, 512, level_smem_, st>>>(dev_, d_small_.p + q0, cnt, d_big_.p + b0, ntz,
                                                                             d_y_, d_z_);
-            if (bc > 0)
-                mf::k_wide_bwd_x<T><<<dim3(ntz, bc), 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
+            if (bc > 0) {
+                const int mnc = S.ncol[big_list_[b0]], g = mf::fwd_group(mnc), cpc = 16 * (32 / g);
+                const dim3 gx((mnc + cpc - 1) / cpc, bc);
+                if (g == 8) mf::k_wide_bwd_x<T, 8><<<gx, 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
+                else if (g == 16) mf::k_wide_bwd_x<T, 16><<<gx, 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
+                else mf::k_wide_bwd_x<T, 32><<<gx, 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
+            }
         }
     }
 

@@ -305,6 +305,11 @@ struct Forging3D {
     // off in the reference's FP64 form, whose iteration counts it must reproduce)
     bool pcg_early_abort = false;
     double pcg_budget_scale = 2.0;  // factorisations' worth of PCG iterations a reused factor may take
+    // Inexact Newton (off by default; the reference solves every linear system to 1e-7): with pcg_forcing f > 0 a
+    // Newton iteration's PCG stops at the relative residual f x the previous iteration's update norm, clamped to
+    // [1e-7, 1e-3] (1e-3 for the first iteration of an increment)
+    double pcg_forcing = 0;
+    double lin_tol = 1e-7;  // the PCG tolerance of the linear solve in progress
     int factor_step = -1, stale_failures = 0;  // increment of the cached factor; failed tries of a stale one
     int wide_rows = mf::kWideM;  // fronts at least this tall use the multi-CTA solve path
     // learned warm start: mode bit 1 records (inputs, target) of every accepted increment into the network's
@@ -535,7 +540,9 @@ struct Forging3D {
         ahead_t = t;
         ahead_onx = onx;
         ahead_ony = ony;
-        topo_ahead.reset(new TetTopology);
+        // the topology replaced at the last remesh is rebuilt in place: its buffers (the 3 x 3 block pattern is a few
+        // hundred MB on a 200k-tet mesh) are reused instead of being allocated and faulted in again
+        if (!topo_ahead) topo_ahead.reset(new TetTopology);
         topo_promise = std::promise<std::string>();
         topo_ready = topo_promise.get_future();
         ahead_pending = true;
@@ -969,7 +976,7 @@ struct Forging3D {
             int its;
             {
                 PhaseTimer pt(t_pcg);
-                its = pcg(b, x, 1e-7, pcg_budget());
+                its = pcg(b, x, lin_tol, pcg_budget());
             }
             if (stale) stale_failures = its >= 0 ? 0 : stale_failures + 1;
             if (its >= 0) {
@@ -1014,7 +1021,7 @@ struct Forging3D {
             // FP64 refinement of the single-precision factor's solution, to the tolerance of the reused-factor PCG
             PhaseTimer pt(t_pcg);
             int l0 = lin_its;
-            int its = pcg(b, x, 1e-7, P.pcg_budget);
+            int its = pcg(b, x, lin_tol, P.pcg_budget);
             refine_its += lin_its - l0;
             if (its < 0) {
                 have_factor = false;
@@ -1047,6 +1054,7 @@ struct Forging3D {
                 View3 V = view();
                 k_regularise<<<grid(n), 256, 0, st>>>(V);
             }
+            lin_tol = pcg_forcing > 0 ? rclamp(pcg_forcing * last_rel, 1e-7, 1e-3) : 1e-7;
             solve_linear(d_b, d_dv);
             // slope = sum R.dv with R fixed-zeroed (= -b.dv), and |dv|^2
             double dvdv = 0;
@@ -1463,7 +1471,7 @@ struct Forging3D {
         S("factor_fp32", lin->value_bytes() == 4) S("fp32_fallbacks", fp32_fallbacks) S("refine_its", refine_its)
         S("pcg_early_abort", pcg_early_abort) S("pcg_failures_total", pcg_failures_total) S("wide_front_rows", wide_rows) S("tc_updates", lin->tc_launches())
         S("factor_gflop", factor_gflop())
-        S("pcg_budget_now", pcg_budget()) S("pcg_budget_scale", pcg_budget_scale)
+        S("pcg_budget_now", pcg_budget()) S("pcg_budget_scale", pcg_budget_scale) S("pcg_forcing", pcg_forcing)
         S("ws_used", ws_used) S("ws_fallbacks", ws_fallbacks) S("ws_mode", ws_mode) S("ws_policy", ws_policy) S("ws_smooth", ws_smooth)
         S("ws_last_step", ws_last_step)
         S("remesh", remesh_enabled) S("remesh_count", remesh_count) S("remesh_rejected", remesh_rejected)
@@ -1495,6 +1503,10 @@ struct Forging3D {
         else if (nm == "pcg_budget_scale") {
             if (!(v > 0 && v <= 16)) throw Failure(IFEA_INPUT_INVALID, "pcg_budget_scale must lie in (0, 16]");
             pcg_budget_scale = v;
+        }
+        else if (nm == "pcg_forcing") {
+            if (!(v >= 0 && v <= 1)) throw Failure(IFEA_INPUT_INVALID, "pcg_forcing must lie in [0, 1]");
+            pcg_forcing = v;
         }
         else if (nm == "remesh") remesh_enabled = v != 0;
         else if (nm == "ws_smooth") ws_smooth = std::max(0, (int)v);
