@@ -642,21 +642,38 @@ __device__ __forceinline__ T group_dot(const T *__restrict__ row, const T *__res
     return acc;
 }
 
-// Lanes per row of the forward GEMVs of a level whose longest row has `len` entries.
-inline int fwd_group(int len) { return len <= 96 ? 8 : len <= 224 ? 16 : 32; }
+// Lanes per row (or column) of a wide front's pivot-block and L21 GEMVs whose rows have at most `len` entries.
+__host__ __device__ inline int fwd_group(int len) { return len <= 96 ? 8 : len <= 224 ? 16 : 32; }
+
+// Work lists of the wide fronts' solve kernels: per kind and level, (front, tile) pairs, a front's tiles in
+// order, the fronts of a level by descending pivot count. A CTA takes one pair, so no CTA of a launch is idle
+// however unequal the level's fronts.
+enum WideTileKind { kTileFwdY = 0, kTileFwdT = 1, kTileBwdX = 2, kTileBwdZ = 3, kTileAcc = 4, kTileKinds = 5 };
+
+// tiles of front (nc pivots, m rows) for each kind, for 512-thread CTAs
+__host__ __device__ inline int wide_tiles(int kind, int nc, int m)
+{
+    const int per = 16 * (32 / fwd_group(nc));
+    switch (kind) {
+    case kTileFwdY:
+    case kTileBwdX: return (nc + per - 1) / per;
+    case kTileFwdT: return (m - nc + per - 1) / per;
+    case kTileBwdZ: return (nc + 15) / 16;
+    default: return (m + 511) / 512;
+    }
+}
 
 // y1 = X acc1 (X lower triangular, read through its mirror: row r is X(c, r) for c <= r, contiguous), G lanes
-// per row, 16 * 32 / G rows per CTA counted from the bottom (longest rows first)
+// per row, 16 * 32 / G rows per tile counted from the bottom (longest rows first)
 template <typename T, int G>
-static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32_t *__restrict__ fronts, T *y, T *Y1)
+__device__ __forceinline__ void dev_wide_fwd_y(Dev<T> D, int s, int tile, T *y, T *Y1)
 {
     constexpr int RPC = 16 * (32 / G);
-    const int s = fronts[blockIdx.y];
     const int nc = D.ncol[s], c0 = D.c0[s], ntile = (nc + RPC - 1) / RPC;
-    if ((int)blockIdx.x >= ntile) return;
-    const int lane = threadIdx.x & 31;
-    const int r = (ntile - 1 - blockIdx.x) * RPC + (threadIdx.x >> 5) * (32 / G) + lane / G;
-    if ((threadIdx.x >> 5) * (32 / G) + (ntile - 1 - blockIdx.x) * RPC >= nc) return;  // the warp's first row
+    if (tile >= ntile) return;
+    const int lane = threadIdx.x & 31, w0 = (ntile - 1 - tile) * RPC + (threadIdx.x >> 5) * (32 / G);
+    if (w0 >= nc) return;  // the warp's first row
+    const int r = w0 + lane / G;
     const bool ok = r < nc;
     const T v = group_dot<G>(D.Xinv + D.xinv_off[s] + (int64_t)(ok ? r : 0) * nc, D.Abig + D.idx_start[s],
                              ok ? r + 1 : 0, lane % G);
@@ -665,21 +682,37 @@ static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32
         Y1[D.idx_start[s] + r] = v;
     }
 }
+template <typename T>
+static __global__ void __launch_bounds__(512) k_wide_fwd_y(Dev<T> D, const int32_t *__restrict__ tiles, T *y, T *Y1)
+{
+    const int s = tiles[2 * blockIdx.x], tile = tiles[2 * blockIdx.x + 1], g = fwd_group(D.ncol[s]);
+    if (g == 8) dev_wide_fwd_y<T, 8>(D, s, tile, y, Y1);
+    else if (g == 16) dev_wide_fwd_y<T, 16>(D, s, tile, y, Y1);
+    else dev_wide_fwd_y<T, 32>(D, s, tile, y, Y1);
+}
 
-// update vector t = -acc2 + L21 y1 (L21 through its mirror: row i is F(k, nc + i), k < nc), G lanes per row
+// update vector t = -acc2 + L21 y1 (L21 through its mirror: row i is F(k, nc + i), k < nc), G lanes per row,
+// 16 * 32 / G rows per tile
 template <typename T, int G>
-static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32_t *__restrict__ fronts, const T *Y1)
+__device__ __forceinline__ void dev_wide_fwd_t(Dev<T> D, int s, int tile, const T *Y1)
 {
     constexpr int RPC = 16 * (32 / G);
-    const int s = fronts[blockIdx.y];
     const int ms = D.m[s], nc = D.ncol[s], nr = ms - nc;
-    const int lane = threadIdx.x & 31, w0 = blockIdx.x * RPC + (threadIdx.x >> 5) * (32 / G);
+    const int lane = threadIdx.x & 31, w0 = tile * RPC + (threadIdx.x >> 5) * (32 / G);
     if (w0 >= nr) return;  // the warp's first row
     const int i = w0 + lane / G;
     const bool ok = i < nr;
     const T v = group_dot<G>(D.F + D.front_off[s] + (int64_t)(nc + (ok ? i : 0)) * ms, Y1 + D.idx_start[s],
                              ok ? nc : 0, lane % G);
     if (ok && lane % G == 0) D.U[D.uvec_start[s] + i] = -D.Abig[D.idx_start[s] + nc + i] + v;
+}
+template <typename T>
+static __global__ void __launch_bounds__(512) k_wide_fwd_t(Dev<T> D, const int32_t *__restrict__ tiles, const T *Y1)
+{
+    const int s = tiles[2 * blockIdx.x], tile = tiles[2 * blockIdx.x + 1], g = fwd_group(D.ncol[s]);
+    if (g == 8) dev_wide_fwd_t<T, 8>(D, s, tile, Y1);
+    else if (g == 16) dev_wide_fwd_t<T, 16>(D, s, tile, Y1);
+    else dev_wide_fwd_t<T, 32>(D, s, tile, Y1);
 }
 
 // z = y1 - L21^T x2, one warp per pivot column; x2 is read through the front's row indices as the column
@@ -725,10 +758,13 @@ __device__ __forceinline__ void dev_wide_bwd_x(Dev<T> D, int s, int tile, const 
     for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (ok && lane % G == 0) x[c0 + j] = v;
 }
-template <typename T, int G>
-static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev<T> D, const int32_t *__restrict__ fronts, const T *Z, T *x)
+template <typename T>
+static __global__ void __launch_bounds__(512) k_wide_bwd_x(Dev<T> D, const int32_t *__restrict__ tiles, const T *Z, T *x)
 {
-    dev_wide_bwd_x<T, G>(D, fronts[blockIdx.y], blockIdx.x, Z, x);
+    const int s = tiles[2 * blockIdx.x], tile = tiles[2 * blockIdx.x + 1], g = fwd_group(D.ncol[s]);
+    if (g == 8) dev_wide_bwd_x<T, 8>(D, s, tile, Z, x);
+    else if (g == 16) dev_wide_bwd_x<T, 16>(D, s, tile, Z, x);
+    else dev_wide_bwd_x<T, 32>(D, s, tile, Z, x);
 }
 
 // Trailing update of every listed front by its pivot columns [k0, k0 + kd), kd = min(kdepth, ncol - k0):
@@ -1246,25 +1282,26 @@ __device__ __forceinline__ void dev_backward(Dev<T> D, int s, const T *y, T *x)
 // coming down).
 template <typename T>
 static __global__ void __launch_bounds__(512) k_fwd_level(Dev<T> D, const int32_t *__restrict__ small, int nsmall,
-                                                          const int32_t *__restrict__ big, int nacc, T *y)
+                                                          const int32_t *__restrict__ tiles, T *y)
 {
     if ((int)blockIdx.x < nsmall) {
         dev_forward(D, small[blockIdx.x], y);
     } else {
-        int t = blockIdx.x - nsmall;  // nacc CTAs per wide front share its rows
-        dev_wide_acc(D, big[t / nacc], y, t % nacc, nacc);
+        // a wide front's rows are shared by ceil(m / 512) CTAs, one tile each
+        const int t = blockIdx.x - nsmall, s = tiles[2 * t];
+        dev_wide_acc(D, s, y, tiles[2 * t + 1], (D.m[s] + blockDim.x - 1) / blockDim.x);
     }
 }
 
 template <typename T>
 static __global__ void __launch_bounds__(512) k_bwd_level(Dev<T> D, const int32_t *__restrict__ small, int nsmall,
-                                                          const int32_t *__restrict__ big, int ntz, T *x, T *Z)
+                                                          const int32_t *__restrict__ tiles, T *x, T *Z)
 {
     if ((int)blockIdx.x < nsmall) {
         dev_backward(D, small[blockIdx.x], x, x);
     } else {
-        int t = blockIdx.x - nsmall;
-        dev_wide_bwd_z(D, big[t / ntz], t % ntz, x, Z);
+        const int t = blockIdx.x - nsmall;
+        dev_wide_bwd_z(D, tiles[2 * t], tiles[2 * t + 1], x, Z);
     }
 }
 
@@ -1497,6 +1534,27 @@ public:
                              [&](int a, int b) { return S.ncol[a] > S.ncol[b]; });
         d_big_.upload(big_list_, st_);
         {
+            // the solve kernels' work lists (pairs (front, tile), kinds x levels)
+            const int nl1 = S.nlevels + 1;
+            std::vector<int32_t> wt;
+            wt_start_.assign(mf::kTileKinds * nl1, 0);
+            for (int kind = 0; kind < mf::kTileKinds; kind++) {
+                for (int l = 0; l < S.nlevels; l++) {
+                    wt_start_[kind * nl1 + l] = (int32_t)(wt.size() / 2);
+                    for (int q = big_start_[l]; q < big_start_[l + 1]; q++) {
+                        const int sn = big_list_[q], nt = mf::wide_tiles(kind, S.ncol[sn], S.m[sn]);
+                        for (int t = 0; t < nt; t++) {
+                            wt.push_back(sn);
+                            wt.push_back(t);
+                        }
+                    }
+                }
+                wt_start_[kind * nl1 + S.nlevels] = (int32_t)(wt.size() / 2);
+            }
+            if (wt.empty()) wt.assign(2, 0);
+            d_wtiles_.upload(wt, st_);
+        }
+        {
             std::vector<int64_t> ts(big_list_.size() + 1, 0);
             for (size_t q = 0; q < big_list_.size(); q++) {
                 int sn = big_list_[q], nc = S.ncol[sn], nr = S.m[sn] - nc, tk = (nc + 31) / 32, tr = (nr + 31) / 32;
@@ -1508,9 +1566,7 @@ public:
         wide_smem_ = 8;
         for (int sn : big_list_) wide_smem_ = std::max(wide_smem_, (size_t)std::max(S.ncol[sn], S.m[sn] - S.ncol[sn]) * sizeof(T));
         if (wide_smem_ > 200 * 1024) throw Failure(IFEA_INPUT_INVALID, "front larger than the wide solve kernels' shared-memory window");
-        ensure_dynamic_smem((const void *)mf::k_wide_bwd_x<T, 8>, (int)wide_smem_);
-        ensure_dynamic_smem((const void *)mf::k_wide_bwd_x<T, 16>, (int)wide_smem_);
-        ensure_dynamic_smem((const void *)mf::k_wide_bwd_x<T, 32>, (int)wide_smem_);
+        ensure_dynamic_smem((const void *)mf::k_wide_bwd_x<T>, (int)wide_smem_);
         // inverse passes of the wide supernodes, per level: diagonal copies, then for groups of 2, 4, ... blocks
         // the T pass and the X21 pass, each followed by its reduction when a block range was split
         std::vector<mf::XTask> tasks;
@@ -1869,49 +1925,30 @@ public:
     void enqueue_sweeps(cudaStream_t st)
     {
         const MfSymbolic &S = sym_;
+        const int nl1 = S.nlevels + 1;
+        // pairs [first, first + count) of kind k at level l in the work lists
+        auto tiles = [&](int k, int l, int &count) {
+            count = wt_start_[k * nl1 + l + 1] - wt_start_[k * nl1 + l];
+            return d_wtiles_.p + 2 * (int64_t)wt_start_[k * nl1 + l];
+        };
+        int n;
         for (int l = 0; l < S.nlevels; l++) {
             int q0 = small_start_[l], cnt = small_start_[l + 1] - q0;
-            int b0 = big_start_[l], bc = big_start_[l + 1] - b0;
-            int nacc = 1;
-            for (int q = b0; q < b0 + bc; q++) nacc = std::max(nacc, (S.m[big_list_[q]] + 511) / 512);
-            if (cnt + bc > 0)
-                mf::k_fwd_level<T><<<cnt + bc * nacc, 512, small_smem_, st>>>(dev_, d_small_.p + q0, cnt, d_big_.p + b0,
-                                                                           nacc, d_y_);
-            if (bc > 0) {
-                int mnc = 1, mnr = 1;
-                for (int q = b0; q < b0 + bc; q++) {
-                    mnc = std::max(mnc, S.ncol[big_list_[q]]);
-                    mnr = std::max(mnr, S.m[big_list_[q]] - S.ncol[big_list_[q]]);
-                }
-                // short rows (the lower levels' pivot counts) share a warp: G lanes per row, 16 * 32 / G rows per CTA
-                const int g = mf::fwd_group(mnc), rpc = 16 * (32 / g);
-                const dim3 gy((mnc + rpc - 1) / rpc, bc), gt((mnr + rpc - 1) / rpc, bc);
-                if (g == 8) {
-                    mf::k_wide_fwd_y<T, 8><<<gy, 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
-                    mf::k_wide_fwd_t<T, 8><<<gt, 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
-                } else if (g == 16) {
-                    mf::k_wide_fwd_y<T, 16><<<gy, 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
-                    mf::k_wide_fwd_t<T, 16><<<gt, 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
-                } else {
-                    mf::k_wide_fwd_y<T, 32><<<gy, 512, 0, st>>>(dev_, d_big_.p + b0, d_y_, d_y1_);
-                    mf::k_wide_fwd_t<T, 32><<<gt, 512, 0, st>>>(dev_, d_big_.p + b0, d_y1_);
-                }
-            }
+            const int32_t *acc = tiles(mf::kTileAcc, l, n);
+            if (cnt + n > 0)
+                mf::k_fwd_level<T><<<cnt + n, 512, small_smem_, st>>>(dev_, d_small_.p + q0, cnt, acc, d_y_);
+            const int32_t *ty = tiles(mf::kTileFwdY, l, n);
+            if (n > 0) mf::k_wide_fwd_y<T><<<n, 512, 0, st>>>(dev_, ty, d_y_, d_y1_);
+            const int32_t *tt = tiles(mf::kTileFwdT, l, n);
+            if (n > 0) mf::k_wide_fwd_t<T><<<n, 512, 0, st>>>(dev_, tt, d_y1_);
         }
         for (int l = S.nlevels - 1; l >= 0; l--) {
             int q0 = small_start_[l], cnt = small_start_[l + 1] - q0;
-            int b0 = big_start_[l], bc = big_start_[l + 1] - b0;
-            int ntz = bc > 0 ? (S.ncol[big_list_[b0]] + 15) / 16 : 1;
-            if (cnt + bc > 0)
-                mf::k_bwd_level<T><<<cnt + bc * ntz, 512, level_smem_, st>>>(dev_, d_small_.p + q0, cnt, d_big_.p + b0, ntz,
-                                                                            d_y_, d_z_);
-            if (bc > 0) {
-                const int mnc = S.ncol[big_list_[b0]], g = mf::fwd_group(mnc), cpc = 16 * (32 / g);
-                const dim3 gx((mnc + cpc - 1) / cpc, bc);
-                if (g == 8) mf::k_wide_bwd_x<T, 8><<<gx, 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
-                else if (g == 16) mf::k_wide_bwd_x<T, 16><<<gx, 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
-                else mf::k_wide_bwd_x<T, 32><<<gx, 512, wide_smem_, st>>>(dev_, d_big_.p + b0, d_z_, d_y_);
-            }
+            const int32_t *tz = tiles(mf::kTileBwdZ, l, n);
+            if (cnt + n > 0)
+                mf::k_bwd_level<T><<<cnt + n, 512, level_smem_, st>>>(dev_, d_small_.p + q0, cnt, tz, d_y_, d_z_);
+            const int32_t *tx = tiles(mf::kTileBwdX, l, n);
+            if (n > 0) mf::k_wide_bwd_x<T><<<n, 512, wide_smem_, st>>>(dev_, tx, d_z_, d_y_);
         }
     }
 
@@ -1960,6 +1997,7 @@ private:
     cusolverSpHandle_t hsp_ = nullptr;
     std::vector<int64_t> inv_off_, xinv_off_;
     std::vector<int32_t> small_start_, small_list_, big_start_, big_list_;
+    std::vector<int32_t> wt_start_;  // work-list offsets of the wide solve kernels, kind x (levels + 1)
     std::vector<int> xinv_pass_start_, xinv_task_start_, xinv_pass_kind_;
     DBuf<mf::XTask> d_xinv_tasks_;
     DBuf<T> d_xinv_w_;
@@ -1968,7 +2006,7 @@ private:
     DBuf<int64_t> d_inv_off_, d_xinv_off_;
     DBuf<int64_t> d_mirror_ts_;   // the wide fronts' mirror tiles, prefix per front
     int64_t mirror_tiles_ = 0;
-    DBuf<int32_t> d_small_, d_big_, d_gst_, d_gsrc_;
+    DBuf<int32_t> d_small_, d_big_, d_gst_, d_gsrc_, d_wtiles_;
     DBuf<T> d_Inv_, d_Xinv_, d_Abig_, d_y1_, d_z_;
     cusparseMatDescr_t descr_ = nullptr;
     MfSymbolic sym_;

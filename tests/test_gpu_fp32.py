@@ -59,14 +59,18 @@ def test_switching_precision_back_restores_the_fp64_path():
     assert abs(info["load"] / ora.scalar("load") - 1) < 1e-6
 
 
-def test_warm_started_fp32_form_meets_the_error_targets_against_a_tight_oracle():
+@pytest.mark.parametrize("forcing", [0.0, 0.05])
+def test_warm_started_fp32_form_meets_the_error_targets_against_a_tight_oracle(forcing):
     # the form bench.py times: extrapolated start (the reference's ExtrapolateStart), Newton tolerance 2e-4, FP32
-    # factor with FP64 refinement; compared with the oracle converged to 1e-6, against the published targets
-    # (ram load within 0.5 %, velocity within 1e-3 relative L2)
+    # factor with FP64 refinement, and (forcing 0.05) each Newton iteration's PCG stopped at 0.05 x the previous
+    # update norm; compared with the oracle converged to 1e-6, against the published targets (ram load within
+    # 0.5 %, velocity within 1e-3 relative L2)
     mesh, dies = upset_case_3d(12.0, 24.0, 1.6, 14.0, seed=4)
     base = dict(C=150, N=0.1, M=0.12, eps0=0.01, friction=0.4, ram=10, h=1.6, ds=0.32, size=24.0)
     gpu = Forging3DSolver(Forging3DConfig(**base, tol=2e-4, extrapolate_start=True), mesh, dies)
     gpu.set_scalar("factor_fp32", 1)
+    gpu.set_scalar("pcg_forcing", forcing)
+    assert gpu.scalar("pcg_forcing") == forcing
     ora = Oracle3D(Forging3DConfig(**base, tol=1e-6), mesh, dies)
     for k in range(5):
         info = gpu.step()
