@@ -11,6 +11,7 @@
 #include "remesh.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -20,6 +21,7 @@
 #include <utility>
 
 #include "../../include/ifea_gpu.h"
+#include "host_par.h"
 
 namespace ifea {
 
@@ -88,31 +90,48 @@ struct LightMesh {
         struct F {
             int32_t k0, k1, k2, p, q, r, seq;
         };
-        std::vector<F> faces;
-        faces.reserve((size_t)4 * ne);
+        // faces bucketed by their smallest node (in creation order within a bucket), each bucket sorted by its
+        // other two nodes and creation order on the host's threads; a face met once is a boundary face
+        std::vector<int32_t> fstart(nn + 1, 0);
+        std::vector<F> faces(4 * (size_t)ne);
         for (int e = 0; e < ne; e++) {
             int a = t[4 * e], b = t[4 * e + 1], c = t[4 * e + 2], d = t[4 * e + 3];
             const int tri[4][3] = {{a, c, b}, {a, b, d}, {a, d, c}, {b, c, d}};
             for (int f = 0; f < 4; f++) {
                 int s[3] = {tri[f][0], tri[f][1], tri[f][2]};
                 std::sort(s, s + 3);
-                faces.push_back({s[0], s[1], s[2], tri[f][0], tri[f][1], tri[f][2], (int32_t)faces.size()});
+                faces[4 * (size_t)e + f] = {s[0], s[1], s[2], tri[f][0], tri[f][1], tri[f][2], 4 * e + f};
+                fstart[s[0] + 1]++;
             }
         }
-        std::sort(faces.begin(), faces.end(), [](const F &u, const F &v) {
-            if (u.k0 != v.k0) return u.k0 < v.k0;
-            if (u.k1 != v.k1) return u.k1 < v.k1;
-            if (u.k2 != v.k2) return u.k2 < v.k2;
-            return u.seq < v.seq;
-        });
-        std::vector<F> boundary;
-        for (size_t i = 0; i < faces.size();) {
-            size_t j = i + 1;
-            while (j < faces.size() && faces[j].k0 == faces[i].k0 && faces[j].k1 == faces[i].k1 && faces[j].k2 == faces[i].k2) j++;
-            if (j - i > 2) return false;
-            if (j - i == 1) boundary.push_back(faces[i]);
-            i = j;
+        for (int n = 0; n < nn; n++) fstart[n + 1] += fstart[n];
+        std::vector<F> byk(faces.size());
+        {
+            std::vector<int32_t> at(fstart.begin(), fstart.end() - 1);
+            for (const F &f : faces) byk[at[f.k0]++] = f;
         }
+        std::vector<std::vector<F>> part(par_chunk_count(nn));
+        std::atomic<bool> bad{false};
+        par_chunks(nn, [&](int ti, int n0, int n1) {
+            for (int n = n0; n < n1; n++) {
+                F *b = byk.data() + fstart[n], *e = byk.data() + fstart[n + 1];
+                std::sort(b, e, [](const F &u, const F &v) {
+                    if (u.k1 != v.k1) return u.k1 < v.k1;
+                    if (u.k2 != v.k2) return u.k2 < v.k2;
+                    return u.seq < v.seq;
+                });
+                for (F *i = b; i < e;) {
+                    F *j = i + 1;
+                    while (j < e && j->k1 == i->k1 && j->k2 == i->k2) j++;
+                    if (j - i > 2) bad = true;
+                    else if (j - i == 1) part[ti].push_back(*i);
+                    i = j;
+                }
+            }
+        });
+        if (bad) return false;
+        std::vector<F> boundary;
+        for (auto &v : part) boundary.insert(boundary.end(), v.begin(), v.end());
         std::sort(boundary.begin(), boundary.end(), [](const F &u, const F &v) { return u.seq < v.seq; });
         bface.clear();
         bsym.clear();
