@@ -182,6 +182,21 @@ TetLocator::TetLocator(const std::vector<d3> &x, const std::vector<int32_t> &tet
                 for (int i = i0; i <= i1; i++) act(((size_t)k * ny_ + j) * nx_ + i);
     };
     for (int e = 0; e < ne; e++) each(e, [&](size_t c) { start_[c + 1]++; });
+    // bounding boxes for find(): a point whose barycentric weights are all >= -1e-9 lies within 3e-9 x the tet's
+    // extent of its box; the margin, 1e-4 of a cell, leaves room for the weights' rounding too
+    bb_margin_ = 1e-4 * cell_;
+    bb_.resize(6 * (size_t)ne);
+    parallel_for(ne, [&](int e) {
+        d3 l = x[tets[4 * e]], h = l;
+        for (int a = 1; a < 4; a++) {
+            d3 p = x[tets[4 * e + a]];
+            l = mk3(rmin(l.x, p.x), rmin(l.y, p.y), rmin(l.z, p.z));
+            h = mk3(rmax(h.x, p.x), rmax(h.y, p.y), rmax(h.z, p.z));
+        }
+        double *b = &bb_[6 * (size_t)e];
+        b[0] = l.x - bb_margin_; b[1] = l.y - bb_margin_; b[2] = l.z - bb_margin_;
+        b[3] = h.x + bb_margin_; b[4] = h.y + bb_margin_; b[5] = h.z + bb_margin_;
+    });
     for (size_t c = 0; c < ncell; c++) start_[c + 1] += start_[c];
     items_.assign(start_[ncell], 0);
     std::vector<int32_t> fill(start_.begin(), start_.end() - 1);
@@ -211,6 +226,8 @@ int TetLocator::find(d3 p, double w[4]) const
     int c = cell_of(p);
     for (int32_t k = start_[c]; k < start_[c + 1]; k++) {
         int e = items_[k];
+        const double *bb = &bb_[6 * (size_t)e];
+        if (p.x < bb[0] || p.y < bb[1] || p.z < bb[2] || p.x > bb[3] || p.y > bb[4] || p.z > bb[5]) continue;
         d3 a = x_[t_[4 * e]], b = x_[t_[4 * e + 1]], cc = x_[t_[4 * e + 2]], d = x_[t_[4 * e + 3]];
         double v = tet_volume(a, b, cc, d);
         if (v <= 0) continue;

@@ -38,6 +38,10 @@ class TetLocator {
     d3 min_;
     int nx_, ny_, nz_;
     std::vector<int32_t> start_, items_, nstart_, nitems_;
+    // each tet's bounding box (min xyz, max xyz), widened by bb_margin_: a point outside it fails the containment
+    // test, so find() skips such candidates before the volume arithmetic and returns the same tet
+    std::vector<double> bb_;
+    double bb_margin_ = 0;
 };
 
 // Isosurface stuffing on the body-centred-cubic lattice of spacing h (IsosurfaceStuffing.Stuff,
