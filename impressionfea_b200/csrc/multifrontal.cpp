@@ -59,11 +59,13 @@ struct CoordNd {
     {
         mark.reset(new SetMark[nb]);
         loc.assign(nb, -1);
-        for (int ax = 0; ax < 3; ax++) {
-            reach[ax].assign(nb, 0.0);
-            for (int v = 0; v < nb; v++)
-                for (int p = gp[v]; p < gp[v + 1]; p++) reach[ax][v] = std::max(reach[ax][v], std::fabs(X(v, ax) - X(gi[p], ax)));
-        }
+        for (int ax = 0; ax < 3; ax++) reach[ax].assign(nb, 0.0);
+        par_chunks(nb, [&](int, int v0, int v1) {
+            for (int ax = 0; ax < 3; ax++)
+                for (int v = v0; v < v1; v++)
+                    for (int p = gp[v]; p < gp[v + 1]; p++)
+                        reach[ax][v] = std::max(reach[ax][v], std::fabs(X(v, ax) - X(gi[p], ax)));
+        });
         std::vector<int> all(nb);
         std::iota(all.begin(), all.end(), 0);
         std::vector<int32_t> perm_rev;  // nodes in reverse elimination order
@@ -286,7 +288,7 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
             for (int b = b0; b < b1; b++) {
                 int d = b * block, c = 0;
                 for (int32_t p = cp[d]; p < cp[d + 1]; p++) {
-                    int o = ri[p] / block;
+                    int o = block == 3 ? ri[p] / 3 : ri[p] / block;  // a constant divisor for the 3D case
                     if (o == b || mark[o] == b) continue;
                     mark[o] = b;
                     part[t].push_back(o);

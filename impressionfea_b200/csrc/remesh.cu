@@ -973,12 +973,21 @@ bool remesh_workpiece(const RemeshInput &in, RemeshOutput &out)
     out.t_refine = seconds_since(t0);
     t0 = std::chrono::steady_clock::now();
     int nn = (int)x.size();
+    if (in.on_topology) {
+        // the caller's work on the final tets (the stepper's topology and analysis) starts here, beside the
+        // surface extraction and placement below; the symmetry-plane flags are LightMesh's
+        std::vector<uint8_t> onx(nn), ony(nn);
+        for (int n = 0; n < nn; n++) {
+            onx[n] = in.sym_x && x[n].x == 0;
+            ony[n] = in.sym_y && x[n].y == 0;
+        }
+        in.on_topology(x, t, onx, ony);
+    }
     LightMesh M;
     if (!M.build(nn, t, x, in.sym_x, in.sym_y)) {
         out.why = "Tetrahedral mesh is not manifold (face shared by more than two tets)";
         return false;
     }
-    if (in.on_topology) in.on_topology(x, t, M.onx, M.ony);
     std::vector<d3> stuffed = x;
     std::vector<uint8_t> contact(nn, IFEA_FREE);
     std::vector<d3> nrm = surface_normals(M, x);

@@ -72,9 +72,10 @@ struct RemeshInput {
     int recovery_pass = 0, refinement_levels = 1, max_nodes = 1 << 30;
     double sig_ref = 0;
     std::vector<HotSpot> hot;
-    // called once the new mesh's connectivity is final (after refinement, before contact placement moves its
-    // nodes): node positions so far, tets, symmetry-plane flags. A caller can start work that needs only the
-    // connectivity (topology, symbolic analysis) while the remesher places and remaps.
+    // called once the new mesh's connectivity is final (after refinement, before the surface is extracted and
+    // contact placement moves its nodes): node positions so far, tets, symmetry-plane flags. A caller can start
+    // work that needs only the connectivity (topology, symbolic analysis) while the remesher places and remaps;
+    // the mesh may still be rejected after the call (not manifold, too poor).
     std::function<void(const std::vector<d3> &, const std::vector<int32_t> &, const std::vector<uint8_t> &,
                        const std::vector<uint8_t> &)>
         on_topology;
