@@ -48,7 +48,7 @@ struct CoordNd {
     const int *gp, *gi;
     const double *x;
     std::unique_ptr<SetMark[]> mark;
-    std::vector<int32_t> loc, vis;
+    std::vector<int32_t> loc;  // position of a node in the V side of the cover being built (-1 elsewhere)
     std::vector<double> reach[3];
     std::atomic<int> stamp{0};
 
@@ -138,7 +138,7 @@ struct CoordNd {
                 if (isR(w) && loc[w] >= 0) adj[i].push_back(loc[w]);
             }
         std::vector<int> mu(U.size(), -1), mv(V.size(), -1);
-        vis.assign(V.size(), -1);
+        std::vector<int32_t> vis(V.size(), -1);  // per call: the two halves of a split cover concurrently
         for (int u = 0; u < (int)U.size(); u++)
             for (int v : adj[u])
                 if (mv[v] < 0) {
@@ -255,7 +255,9 @@ struct CoordNd {
         for (int i = (int)S.size() - 1; i >= 0; i--) perm_rev.push_back(S[i]);
         for (auto &v : arr) std::vector<int>().swap(v);
         std::vector<int>().swap(set);
-        if (depth >= 1 && depth < kParDepth && (int)(L.size() + R.size()) > 4096) {
+        // the halves on two threads: they touch disjoint nodes' marks and cover slots (their neighbours outside
+        // are the separator's, which neither changes), and the right half's order goes first either way
+        if (depth < kParDepth && (int)(L.size() + R.size()) > 4096) {
             std::vector<int32_t> pr, pl;
             std::thread t([&] { split(R, depth + 1, pr); });
             split(L, depth + 1, pl);
