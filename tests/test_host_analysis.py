@@ -64,7 +64,10 @@ def _run(driver, tmp_path, mesh, block, order=None):
 def _cases():
     up_mesh, up_dies = upset_case_3d(10.0, 20.0, 2.0, 12.0, seed=1)
     gb_mesh, gb_dies = gear_blank_case_3d(3.0, seed=2)
-    return {"upset": (up_mesh, up_dies, 2.0, 20.0), "gear_blank": (gb_mesh, gb_dies, 3.0, 50.0)}
+    # 12.6k nodes: above the size from which the topology and analysis passes run on host threads
+    gf_mesh, gf_dies = gear_blank_case_3d(1.2, seed=3)
+    return {"upset": (up_mesh, up_dies, 2.0, 20.0), "gear_blank": (gb_mesh, gb_dies, 3.0, 50.0),
+            "gear_blank_threaded": (gf_mesh, gf_dies, 1.2, 50.0)}
 
 
 CASES = _cases()
