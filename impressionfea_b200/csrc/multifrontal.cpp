@@ -273,7 +273,7 @@ struct CoordNd {
 }  // namespace
 
 std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, int block, void *hsp, void *descr,
-                                const double *node_xyz)
+                                const double *node_xyz, const int32_t *node_start, const int32_t *node_list)
 {
     n = n_;
     if (n <= 0) return "empty system";
@@ -282,7 +282,15 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
 
     // 1. nested dissection of the block graph (no self loops); per chunk of nodes, joined in node order
     std::vector<int> gp(nb + 1, 0), gi;
-    {
+    const bool given = block > 1 && node_start && node_list;  // the node graph from the caller's node lists
+    if (given) {
+        gi.reserve((size_t)node_start[nb]);
+        for (int b = 0; b < nb; b++) {
+            for (int32_t k = node_start[b]; k < node_start[b + 1]; k++)
+                if (node_list[k] != b) gi.push_back(node_list[k]);
+            gp[b + 1] = (int)gi.size();
+        }
+    } else {
         std::vector<std::vector<int>> part(par_chunk_count(nb));
         par_chunks(nb, [&](int t, int b0, int b1) {
             std::vector<int> mark(nb, -1);
@@ -324,7 +332,7 @@ std::string MfSymbolic::analyze(int n_, const int32_t *cp, const int32_t *ri, in
     //     them together, column counts are cc(block k + c) = block cc_node(k) - c, and the supernode test and the
     //     row structures carry over node by node. Otherwise they run on the matrix itself.
     bool nodal = block > 1, sorted_rows = true;
-    if (nodal) {
+    if (nodal && !given) {
         std::atomic<bool> all_nodal{true}, all_sorted{true};
         par_chunks(nb, [&](int, int b0, int b1) {
             bool nodal = true, sorted_rows = true;

@@ -63,8 +63,12 @@ struct MfSymbolic {
     // Full symmetric CSC pattern (both triangles) of an n x n matrix; block = 3 orders 3x3 node blocks together.
     // The node order is METIS nested dissection through cuSOLVER's host helper, or, when node_xyz (3 coordinates
     // per node) is given, this file's coordinate nested dissection (coordinate_nd).
+    // node_start / node_list (block > 1): each node's neighbours, itself included, ascending, for a caller that built
+    // col_ptr / row_idx as the full block x block pattern of exactly these lists with ascending rows (the stepper's
+    // TetTopology): the node graph is read from them and the pattern's node structure is not verified again.
     std::string analyze(int n, const int32_t *col_ptr, const int32_t *row_idx, int block, void *cusolver_sp_handle,
-                        void *mat_descr, const double *node_xyz = nullptr);
+                        void *mat_descr, const double *node_xyz = nullptr, const int32_t *node_start = nullptr,
+                        const int32_t *node_list = nullptr);
 };
 
 }  // namespace ifea

@@ -479,10 +479,12 @@ struct Forging3D {
     {
         const int ndof = tp->ndof;
         const int32_t *cp = tp->col_ptr.data(), *ri = tp->row_idx.data();
-        analysis_job(dev, ndof, cp, ri, xyz, out, err);
+        analysis_job(dev, ndof, cp, ri, xyz, out, err, tp->nbr_start.data(), tp->nbr.data());
     }
+    // the pattern (cp, ri) is the topology's full 3 x 3 block pattern of the node lists (node_start, node_list)
     void analysis_job(int dev, int ndof, const int32_t *cp, const int32_t *ri, const double *xyz,
-                      std::unique_ptr<MfSymbolic> *out, std::string *err)
+                      std::unique_ptr<MfSymbolic> *out, std::string *err, const int32_t *node_start,
+                      const int32_t *node_list)
     {
         cusolverSpHandle_t hsp = nullptr;
         cusparseMatDescr_t descr = nullptr;
@@ -498,7 +500,7 @@ struct Forging3D {
                 cusparseSetMatType(descr, CUSPARSE_MATRIX_TYPE_GENERAL);
                 cusparseSetMatIndexBase(descr, CUSPARSE_INDEX_BASE_ZERO);
                 std::unique_ptr<MfSymbolic> S(new MfSymbolic);
-                std::string e = S->analyze(ndof, cp, ri, 3, hsp, descr, xyz);
+                std::string e = S->analyze(ndof, cp, ri, 3, hsp, descr, xyz, node_start, node_list);
                 if (e.empty())
                     *out = std::move(S);
                 else
@@ -558,12 +560,13 @@ struct Forging3D {
             // the pattern's addresses are taken before set_mesh may swap the topology in (the buffers move with it)
             const int ndof = topo_ahead->ndof;
             const int32_t *cp = topo_ahead->col_ptr.data(), *ri = topo_ahead->row_idx.data();
+            const int32_t *ns = topo_ahead->nbr_start.data(), *nl = topo_ahead->nbr.data();
             topo_promise.set_value(e);
             if (!e.empty()) {
                 sym_err = e;
                 return;
             }
-            analysis_job(dev, ndof, cp, ri, xyz ? ahead_x.data() : nullptr, &sym_pre, &sym_err);
+            analysis_job(dev, ndof, cp, ri, xyz ? ahead_x.data() : nullptr, &sym_pre, &sym_err, ns, nl);
         });
     }
 
