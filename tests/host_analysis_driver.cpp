@@ -65,7 +65,10 @@ int main(int argc, char **argv)
 {
     if (argc == 5 && std::strcmp(argv[1], "quad") == 0) return quad(std::atoi(argv[2]), std::atoi(argv[3]), argv[4]);
     if (argc != 4 && argc != 5) return 2;
-    bool xyz = argc == 5 && std::strcmp(argv[4], "xyz") == 0;
+    // optional 4th argument: "xyz" (coordinate dissection), "lists" (coordinate dissection, the node graph passed
+    // as the topology's node lists)
+    bool lists = argc == 5 && std::strcmp(argv[4], "lists") == 0;
+    bool xyz = lists || (argc == 5 && std::strcmp(argv[4], "xyz") == 0);
     FILE *f = std::fopen(argv[1], "rb");
     if (!f) return 3;
     int32_t hdr[2];
@@ -85,7 +88,7 @@ int main(int argc, char **argv)
     }
     ifea::MfSymbolic S;
     e = S.analyze(topo.ndof, topo.col_ptr.data(), topo.row_idx.data(), std::atoi(argv[3]), nullptr, nullptr,
-                  xyz ? x.data() : nullptr);
+                  xyz ? x.data() : nullptr, lists ? topo.nbr_start.data() : nullptr, lists ? topo.nbr.data() : nullptr);
     if (!e.empty()) {
         std::fprintf(stderr, "symbolic: %s\n", e.c_str());
         return 6;

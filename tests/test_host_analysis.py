@@ -103,6 +103,15 @@ def test_nodal_symbolic_analysis_matches_equation_level(driver, tmp_path, case):
         np.testing.assert_array_equal(nodal[name], eqn[name], err_msg=name)
 
 
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_analysis_from_the_topology_node_lists_matches_the_pattern_scan(driver, tmp_path, case):
+    # the stepper hands its topology's node lists to the analysis instead of the scan of the 3 x 3 block pattern
+    scan = _run(driver, tmp_path, CASES[case][0], 3, "xyz")
+    lists = _run(driver, tmp_path, CASES[case][0], 3, "lists")
+    for name in SYMBOLIC:
+        np.testing.assert_array_equal(lists[name], scan[name], err_msg=name)
+
+
 @pytest.mark.parametrize("order", [None, "xyz"])
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_front_layout_is_self_consistent(driver, tmp_path, case, order):
