@@ -327,7 +327,8 @@ ifea_status ifea_band_factor_solve(int32_t n, int32_t half_bandwidth, double *ba
  * in d_band itself; the only other working memory is a fixed 16-byte device array inside the library holding the
  * two status words, present on every GPU that loads it until the process exits. Every call looks up that array's
  * device address in the current device's context, launches one kernel, copies the status words back and waits
- * for cuda_stream to finish. All calls on a device share the status words; each call re-initialises them, but
+ * for cuda_stream to finish (so it cannot be called while cuda_stream is being captured into a CUDA graph). All
+ * calls on a device share the status words; each call re-initialises them, but
  * calls that overlap on the same GPU race on them and must be serialised by the caller.
  * Returns IFEA_NOT_SPD with *bad_row / *pivot on a non-positive pivot. Allocates nothing. */
 ifea_status ifea_band_factor_solve_noalloc(int32_t n, int32_t half_bandwidth, double *d_band, double *d_rhs,
