@@ -616,7 +616,8 @@ def run_gpu(args, rank, world):
                 "data": "synthetic",
                 "config": config_dict(cfg, mesh, {
                     "form": "learned warm start (per-node MLP, BF16 on tcgen05) + FP32 multifrontal factor with FP64 "
-                            "PCG refinement, Newton tolerance 2e-4 (plain FP64 form: reference start, 1e-3, FP64 direct)",
+                            "PCG refinement, inexact Newton (PCG to 0.05 x the previous update norm), Newton tolerance "
+                            "2e-4 (plain FP64 form: reference start, 1e-3, FP64 direct)",
                     "increments": f"{W + 1}..{W + k}", "l2": "flushed (256 MiB write) between timed increments",
                     "newton_iterations": int(sum(i["iterations"] for i in infos)),
                     "factorisations": int(infos[-1]["n_factor"] - infos[0]["n_factor"]) + 1 if infos else 0,
